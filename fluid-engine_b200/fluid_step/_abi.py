@@ -1,0 +1,281 @@
+"""ctypes mirror of include/fluid_step.h.
+
+Struct layouts, enum values and status codes are declared once here and used
+by the host-side mirror of the reference's ComputeStep API (pipelines.py),
+by the tests and by bench.py.  The shared library is the product; this module
+only loads it and declares its signatures.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
+                    c_int32, c_size_t, c_uint32, c_uint64, c_void_p)
+
+ABI_VERSION = 1
+
+# fe_status
+FE_OK = 0
+FE_ERR_INVALID_ARGUMENT = 1
+FE_ERR_NOT_PREPARED = 2
+FE_ERR_CUDA = 3
+FE_ERR_OUT_OF_MEMORY = 4
+FE_ERR_NON_FINITE = 5
+FE_ERR_ITERATION_CAP = 6
+FE_ERR_TIMEOUT = 7
+FE_ERR_NO_DEVICE = 8
+FE_ERR_CAPACITY = 9
+FE_ERR_UNSUPPORTED = 10
+
+STATUS_NAMES = {
+    0: "FE_OK", 1: "FE_ERR_INVALID_ARGUMENT", 2: "FE_ERR_NOT_PREPARED",
+    3: "FE_ERR_CUDA", 4: "FE_ERR_OUT_OF_MEMORY", 5: "FE_ERR_NON_FINITE",
+    6: "FE_ERR_ITERATION_CAP", 7: "FE_ERR_TIMEOUT", 8: "FE_ERR_NO_DEVICE",
+    9: "FE_ERR_CAPACITY", 10: "FE_ERR_UNSUPPORTED",
+}
+
+# fe_sort_algorithm (sorter.rs:19-23: Bitonic, Radix)
+FE_SORT_BITONIC = 0
+FE_SORT_RADIX = 1
+# fe_mode
+FE_MODE_REFERENCE = 0
+FE_MODE_FIXED = 1
+# fe_solver
+FE_SOLVER_FIXED_ITERS = 0
+FE_SOLVER_TOLERANCE = 1
+# fe_warm_start
+FE_WARM_REFERENCE = 0
+FE_WARM_LEARNED = 1
+
+# fe_field
+FE_FIELD_POSITION_A = 0
+FE_FIELD_POSITION_B = 1
+FE_FIELD_VELOCITY_A = 2
+FE_FIELD_VELOCITY_B = 3
+FE_FIELD_DENSITY = 4
+FE_FIELD_FACTOR = 5
+FE_FIELD_SOURCE_TERM = 6
+FE_FIELD_PRESSURE = 7
+FE_FIELD_PRESSURE_ACCEL = 8
+FE_FIELD_ENTRY_HASH = 9
+FE_FIELD_ENTRY_INDEX = 10
+FE_FIELD_GRID_START = 11
+FE_FIELD_STATS = 12
+
+VEC4_FIELDS = {FE_FIELD_POSITION_A, FE_FIELD_POSITION_B, FE_FIELD_VELOCITY_A,
+               FE_FIELD_VELOCITY_B, FE_FIELD_PRESSURE_ACCEL}
+UINT_FIELDS = {FE_FIELD_ENTRY_HASH, FE_FIELD_ENTRY_INDEX, FE_FIELD_GRID_START,
+               FE_FIELD_STATS}
+TABLE_FIELDS = {FE_FIELD_ENTRY_HASH, FE_FIELD_ENTRY_INDEX, FE_FIELD_GRID_START}
+
+FE_STEP_INIT_NS = 0x1
+FE_STEP_NO_GRAPH = 0x2
+
+FE_STATS_ITERATION_CAP_HIT = 0x1
+FE_STATS_NEIGHBOR_OVERFLOW = 0x2
+FE_STATS_LOOKBACK_TIMEOUT = 0x4
+
+FE_MAX_PARTICLES = 1 << 26
+
+
+class FeParams(Structure):
+    """fe_params: SimulationParams (particle.rs:310-331) + AppUI knobs."""
+    _fields_ = [
+        ("particle_radius", c_float),
+        ("particle_mass", c_float),
+        ("smoothing_radius", c_float),
+        ("target_density", c_float),
+        ("viscosity", c_float),
+        ("relax_factor", c_float),
+        ("dt", c_float),
+        ("density_solver_iterations", c_uint32),
+        ("divergence_solver_iterations", c_uint32),
+        ("gravity", c_float * 3),
+        ("box_min", c_float * 3),
+        ("box_max", c_float * 3),
+        ("grid_res", c_int32 * 3),
+        ("sort_algorithm", c_uint32),
+        ("use_cfl", c_uint32),
+        ("use_solver_error_threshold", c_uint32),
+        ("density_error_pct", c_float),
+        ("divergence_error_pct", c_float),
+        ("cfl_lambda", c_float),
+        ("cfl_min_dt", c_float),
+        ("cfl_max_dt", c_float),
+        ("cfl_growth", c_float),
+        ("mode", c_uint32),
+        ("solver", c_uint32),
+        ("density_tolerance", c_float),
+        ("divergence_tolerance", c_float),
+        ("min_iterations", c_uint32),
+        ("max_iterations", c_uint32),
+        ("warm_start", c_uint32),
+        ("reserved", c_uint32 * 7),
+    ]
+
+
+class FeStats(Structure):
+    """fe_stats: stats_buffer (stats.comp:8) + decoded and FP64 extras."""
+    _fields_ = [
+        ("max_speed_bits", c_uint32),
+        ("density_error_fp", c_uint32),
+        ("divergence_error_fp", c_uint32),
+        ("substeps", c_uint32),
+        ("max_speed", c_float),
+        ("avg_density_error", c_float),
+        ("avg_divergence_error", c_float),
+        ("dt", c_float),
+        ("avg_density_error_f64", c_double),
+        ("avg_divergence_error_f64", c_double),
+        ("density_residual", c_double),
+        ("divergence_residual", c_double),
+        ("density_iterations", c_uint32),
+        ("divergence_iterations", c_uint32),
+        ("total_density_iterations", c_uint64),
+        ("total_divergence_iterations", c_uint64),
+        ("flags", c_uint32),
+        ("reserved", c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: (list(getattr(self, name)) if name == "reserved" else getattr(self, name))
+                for name, _ in self._fields_ if name != "reserved"}
+
+
+def default_params() -> FeParams:
+    """Defaults of Scene::new() (scene.rs:14-86) and AppUI::new() (ui.rs:31-49).
+
+    Pure-Python twin of fe_default_params(), usable without the library.
+    """
+    import numpy as np
+    p = FeParams()
+    radius = np.float32(0.02)
+    spacing = np.float32(radius * np.float32(2.0))
+    p.particle_radius = float(radius)
+    p.particle_mass = float(np.float32(1000.0) * (spacing * spacing * spacing))
+    p.smoothing_radius = float(radius * np.float32(4.0))
+    p.target_density = 1000.0
+    p.viscosity = 0.15
+    p.relax_factor = 0.5
+    p.dt = 0.005
+    p.density_solver_iterations = 4
+    p.divergence_solver_iterations = 4
+    p.gravity[:] = [0.0, -9.81, 0.0]
+    p.box_min[:] = [-1.5, 0.0, -1.0]
+    p.box_max[:] = [0.8, 4.0, 1.0]
+    p.grid_res[:] = [128, 128, 128]
+    p.sort_algorithm = FE_SORT_RADIX
+    p.use_cfl = 0
+    p.use_solver_error_threshold = 0
+    p.density_error_pct = 0.1
+    p.divergence_error_pct = 0.5
+    p.cfl_lambda = 0.4
+    p.cfl_min_dt = 0.001
+    p.cfl_max_dt = 0.05
+    p.cfl_growth = 1.1
+    p.mode = FE_MODE_REFERENCE
+    p.solver = FE_SOLVER_FIXED_ITERS
+    p.density_tolerance = 0.001
+    p.divergence_tolerance = 0.001
+    p.min_iterations = 2
+    p.max_iterations = 100
+    p.warm_start = FE_WARM_REFERENCE
+    return p
+
+
+def copy_params(p: FeParams) -> FeParams:
+    q = FeParams()
+    ctypes.pointer(q)[0] = p
+    return q
+
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PACKAGE_DIR, "libfluidstep.so")
+
+_lib = None
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def load_library(path: str | None = None):
+    """Loads libfluidstep.so from the package directory.
+
+    Raises LibraryMissing when the library was not built: there is no other
+    implementation to fall back to.
+    """
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise LibraryMissing(
+            f"{path} not found: build it with `python fluid-engine_b200/build.py` "
+            "(or __graft_entry__.build()); the DFSPH step has no CPU fallback")
+    lib = ctypes.CDLL(path)
+    _declare(lib)
+    if lib.fe_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"ABI mismatch: library {lib.fe_abi_version()} != {ABI_VERSION}")
+    if path == LIB_PATH:
+        _lib = lib
+    return lib
+
+
+CTX = c_void_p
+
+# name -> (restype, argtypes); mirrors every declaration of fluid_step.h.
+SIGNATURES = {
+    "fe_abi_version": (c_uint32, []),
+    "fe_status_string": (c_char_p, [c_int]),
+    "fe_last_error": (c_char_p, []),
+    "fe_default_params": (None, [POINTER(FeParams)]),
+    "fe_validate_params": (c_int, [POINTER(FeParams)]),
+    "fe_create": (c_int, [POINTER(FeParams), c_uint32, c_void_p, c_void_p, c_int,
+                          POINTER(CTX)]),
+    "fe_destroy": (c_int, [CTX]),
+    "fe_set_params": (c_int, [CTX, POINTER(FeParams)]),
+    "fe_get_params": (c_int, [CTX, POINTER(FeParams)]),
+    "fe_prepare": (c_int, [CTX]),
+    "fe_get_size": (c_int, [CTX, POINTER(c_uint32), POINTER(c_uint32)]),
+    "fe_get_stream": (c_void_p, [CTX]),
+    "fe_synchronize": (c_int, [CTX]),
+    "fe_upload": (c_int, [CTX, c_int, c_void_p, c_size_t]),
+    "fe_download": (c_int, [CTX, c_int, c_void_p, c_size_t]),
+    "fe_neighbor_search": (c_int, [CTX]),
+    "fe_density_alpha": (c_int, [CTX]),
+    "fe_viscosity": (c_int, [CTX]),
+    "fe_density_source": (c_int, [CTX]),
+    "fe_pressure_force": (c_int, [CTX]),
+    "fe_pressure_update": (c_int, [CTX]),
+    "fe_pressure_integration": (c_int, [CTX]),
+    "fe_divergence_source": (c_int, [CTX]),
+    "fe_divergence_integration": (c_int, [CTX]),
+    "fe_stats_pass": (c_int, [CTX]),
+    "fe_read_stats": (c_int, [CTX, POINTER(FeStats)]),
+    "fe_step": (c_int, [CTX, c_uint32, c_uint32, POINTER(FeStats)]),
+    "fe_sort_pairs": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p]),
+    "fe_sort_pairs_host": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int]),
+}
+
+
+def _declare(lib) -> None:
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+class FluidStepError(RuntimeError):
+    """A non-zero fe_status, with the library's last error message."""
+
+    def __init__(self, status: int, where: str, message: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}"
+                         + (f" ({message})" if message else ""))
+
+
+def check(lib, status: int, where: str) -> None:
+    if status != FE_OK:
+        msg = lib.fe_last_error()
+        raise FluidStepError(status, where, msg.decode() if msg else "")

@@ -1,0 +1,329 @@
+/*
+ * fluid_step.h — C ABI of the B200-native DFSPH physics step.
+ *
+ * This header is the drop-in boundary for the compute half of a Fluid-Engine
+ * frame.  The reference drives its physics through the Rust trait
+ * `ComputeStep { load_shader_module, from_pipeline, new, prepare, execute }`
+ * (src/renderer/pipelines/mod.rs:52-76) and the `ComputePipelines` registry
+ * (src/renderer/pipelines/mod.rs:78-124); buffers live in `GpuPhysicsData`
+ * (src/entities/particle.rs:137-308) and parameters in the std140 UBO
+ * `SimulationParams` (src/entities/particle.rs:310-331).  Every entry point
+ * below names the reference item it replaces.
+ *
+ * Conventions
+ *   - Plain C: pointers, sizes and POD structs only.  No C++ or torch types.
+ *   - Every call returns an fe_status and never aborts the process; the
+ *     reference panics instead (e.g. "call prepare() before execute()",
+ *     density_alpha.rs:57), which maps to FE_ERR_NOT_PREPARED here.
+ *   - The library owns all device memory of a context.  Host arrays passed in
+ *     are copied; host arrays passed out are written by the call.
+ *   - Calls on a context enqueue work on that context's CUDA stream, in call
+ *     order, exactly like recording into the reference's command buffer.
+ *     fe_synchronize() waits for it (the reference's fence wait).
+ *   - One context per host thread.  Contexts are independent.
+ */
+#ifndef FLUID_STEP_H
+#define FLUID_STEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FE_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------------- */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------- */
+typedef enum fe_status {
+    FE_OK = 0,
+    FE_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, enum or parameter   */
+    FE_ERR_NOT_PREPARED = 2,     /* execute before prepare                 */
+    FE_ERR_CUDA = 3,             /* a CUDA runtime call failed             */
+    FE_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed               */
+    FE_ERR_NON_FINITE = 5,       /* NaN/Inf found in an input or the state */
+    FE_ERR_ITERATION_CAP = 6,    /* a tolerance solve hit max_iterations   */
+    FE_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up     */
+    FE_ERR_NO_DEVICE = 8,        /* no CUDA device / wrong architecture    */
+    FE_ERR_CAPACITY = 9,         /* a size exceeds a documented maximum    */
+    FE_ERR_UNSUPPORTED = 10      /* combination of options not supported   */
+} fe_status;
+
+/* Sort choice; same order as `enum SortAlgorithm { Bitonic, Radix }`
+ * (src/renderer/pipelines/sorter.rs:19-23). */
+typedef enum fe_sort_algorithm {
+    FE_SORT_BITONIC = 0,
+    FE_SORT_RADIX = 1
+} fe_sort_algorithm;
+
+/* Buffer pairing of the substep.
+ * FE_MODE_REFERENCE reproduces the reference's bindings exactly, including
+ * divergence_source_term / divergence_integration reading `velocity_a` in
+ * the previous sort order (divergence_source_term.rs:47,
+ * divergence_integration.rs:49-50).
+ * FE_MODE_FIXED pairs every velocity with its own particle: the divergence
+ * pass reads and corrects `velocity_b` (the re-sorted copy), and pressures
+ * are carried through the re-sort. */
+typedef enum fe_mode {
+    FE_MODE_REFERENCE = 0,
+    FE_MODE_FIXED = 1
+} fe_mode;
+
+/* Jacobi iteration control.
+ * FE_SOLVER_FIXED_ITERS runs density/divergence_solver_iterations (or the
+ * early-exit choice of renderer/mod.rs:247-265 when
+ * use_solver_error_threshold is set), as the reference does.
+ * FE_SOLVER_TOLERANCE iterates on the GPU until the FP64 average predicted
+ * density error (resp. divergence error) is within tolerance, with
+ * min_iterations..max_iterations bounds.  No reference counterpart. */
+typedef enum fe_solver {
+    FE_SOLVER_FIXED_ITERS = 0,
+    FE_SOLVER_TOLERANCE = 1
+} fe_solver;
+
+/* Initial pressure of each solve. */
+typedef enum fe_warm_start {
+    FE_WARM_REFERENCE = 0, /* density solve from 0, divergence solve from the
+                              density solve's pressures (as the reference) */
+    FE_WARM_LEARNED = 1    /* both solves start from the learned MLP κ    */
+} fe_warm_start;
+
+/* ------------------------------------------------------------------------- */
+/* Parameters                                                                */
+/* ------------------------------------------------------------------------- */
+/* The first block mirrors `SimulationParams` field for field
+ * (src/entities/particle.rs:310-331, shaders/include/common.glsl:11-28);
+ * the padding and the w lanes of the vec4s are dropped.  The second block
+ * mirrors the frame-driver knobs of `AppUI` (src/renderer/ui.rs:12-49) and
+ * the CFL constants of renderer/mod.rs:238-245.  The third block holds this
+ * library's extensions. */
+typedef struct fe_params {
+    /* SimulationParams */
+    float particle_radius;
+    float particle_mass;
+    float smoothing_radius;
+    float target_density;
+    float viscosity;
+    float relax_factor;
+    float dt;
+    uint32_t density_solver_iterations;
+    uint32_t divergence_solver_iterations;
+    float gravity[3];
+    float box_min[3];
+    float box_max[3];
+    int32_t grid_res[3];
+    /* AppUI / frame driver */
+    uint32_t sort_algorithm;             /* fe_sort_algorithm                  */
+    uint32_t use_cfl;                    /* adaptive dt from previous v_max     */
+    uint32_t use_solver_error_threshold; /* early exit: 2 / 1 iterations        */
+    float density_error_pct;             /* η  in % of ρ0 (ui.rs:41, 0.1)       */
+    float divergence_error_pct;          /* ηv in % of ρ0 (ui.rs:42, 0.5)       */
+    float cfl_lambda;                    /* 0.4   (mod.rs:240)                  */
+    float cfl_min_dt;                    /* 0.001 (mod.rs:240)                  */
+    float cfl_max_dt;                    /* 0.05  (mod.rs:240)                  */
+    float cfl_growth;                    /* 1.1   (mod.rs:242)                  */
+    /* extensions */
+    uint32_t mode;                       /* fe_mode                             */
+    uint32_t solver;                     /* fe_solver                           */
+    float density_tolerance;             /* fraction of ρ0, e.g. 0.001 = 0.1 %  */
+    float divergence_tolerance;          /* fraction of ρ0 per dt               */
+    uint32_t min_iterations;             /* tolerance solver lower bound (2)    */
+    uint32_t max_iterations;             /* tolerance solver cap (100)          */
+    uint32_t warm_start;                 /* fe_warm_start                       */
+    uint32_t reserved[7];                /* must be zero                        */
+} fe_params;
+
+/* Per-frame statistics.  The first three words are the reference's
+ * fixed-point `stats_buffer` (stats.comp:8,14-29); the decoded floats follow
+ * renderer/mod.rs:231-236; the FP64 means and solver counters are
+ * extensions. */
+typedef struct fe_stats {
+    uint32_t max_speed_bits;        /* atomicMax of floatBitsToUint(|v|)    */
+    uint32_t density_error_fp;      /* Σ min(uint(|ρ-ρ0|·1), 10000)         */
+    uint32_t divergence_error_fp;   /* Σ min(uint(|s|·10), 10000)           */
+    uint32_t substeps;              /* substeps run by the last fe_step      */
+    float max_speed;                /* from max_speed_bits                   */
+    float avg_density_error;        /* density_error_fp / (1 · N)            */
+    float avg_divergence_error;     /* divergence_error_fp / (10 · N)        */
+    float dt;                       /* dt used by the last substep           */
+    double avg_density_error_f64;   /* mean |ρ-ρ0| in FP64                   */
+    double avg_divergence_error_f64;/* mean |s| in FP64                      */
+    double density_residual;        /* tolerance metric at exit, last solve  */
+    double divergence_residual;     /* (fraction of ρ0)                      */
+    uint32_t density_iterations;    /* Jacobi iterations of the last substep */
+    uint32_t divergence_iterations;
+    uint64_t total_density_iterations;
+    uint64_t total_divergence_iterations;
+    uint32_t flags;                 /* FE_STATS_* bits                        */
+    uint32_t reserved;
+} fe_stats;
+
+#define FE_STATS_ITERATION_CAP_HIT   0x1u /* a tolerance solve hit the cap   */
+#define FE_STATS_NEIGHBOR_OVERFLOW   0x2u /* some particle exceeded the list */
+#define FE_STATS_LOOKBACK_TIMEOUT    0x4u /* a bounded device wait gave up   */
+
+/* Fields addressable by fe_upload / fe_download.  Names follow
+ * `GpuPhysicsData` (particle.rs:137-161).  Vector fields travel as 4 floats
+ * per particle (x, y, z, w) like the reference's vec4 buffers. */
+typedef enum fe_field {
+    FE_FIELD_POSITION_A = 0,    /* float4[N]                                 */
+    FE_FIELD_POSITION_B = 1,    /* float4[N] (sorted copy)                   */
+    FE_FIELD_VELOCITY_A = 2,    /* float4[N]                                 */
+    FE_FIELD_VELOCITY_B = 3,    /* float4[N]                                 */
+    FE_FIELD_DENSITY = 4,       /* float[N]                                  */
+    FE_FIELD_FACTOR = 5,        /* float[N]  (α)                             */
+    FE_FIELD_SOURCE_TERM = 6,   /* float[N]                                  */
+    FE_FIELD_PRESSURE = 7,      /* float[N]  (κ)                             */
+    FE_FIELD_PRESSURE_ACCEL = 8,/* float4[N]                                 */
+    FE_FIELD_ENTRY_HASH = 9,    /* uint32[T] grid_entries[].hash             */
+    FE_FIELD_ENTRY_INDEX = 10,  /* uint32[T] grid_entries[].index            */
+    FE_FIELD_GRID_START = 11,   /* uint32[T]                                 */
+    FE_FIELD_STATS = 12,        /* uint32[3] stats_buffer                    */
+    FE_FIELD_COUNT = 13
+} fe_field;
+
+/* Step flags for fe_step. */
+#define FE_STEP_INIT_NS      0x1u /* neighbour search + density/α first
+                                     (convergence_benchmark.rs:121-124)     */
+#define FE_STEP_NO_GRAPH     0x2u /* launch eagerly instead of via a graph  */
+
+typedef struct fe_ctx fe_ctx;
+
+/* ------------------------------------------------------------------------- */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------- */
+/* ABI version of the loaded library (FE_ABI_VERSION). */
+uint32_t fe_abi_version(void);
+
+/* Text of a status code.  Static storage. */
+const char* fe_status_string(fe_status status);
+
+/* Last error message recorded on this host thread (empty if none). */
+const char* fe_last_error(void);
+
+/* Defaults of `Scene::new()` (src/core/scene.rs:14-86) and `AppUI::new()`
+ * (src/renderer/ui.rs:31-49), plus the extension defaults. */
+void fe_default_params(fe_params* out);
+
+/* Validates a parameter block (finite values, h > 0, mass > 0, box_min <
+ * box_max, iteration bounds, enums).  The reference has no validation. */
+fe_status fe_validate_params(const fe_params* params);
+
+/* ------------------------------------------------------------------------- */
+/* Context = GpuPhysicsData + ComputePipelines                               */
+/* ------------------------------------------------------------------------- */
+/* Creates the device buffers of `GpuPhysicsData::new` (particle.rs:164-299)
+ * for n particles on CUDA device `device`: positions from pos_xyz (3 floats
+ * per particle, w set to 1), velocities from vel_xyz (may be NULL: zero, as
+ * particle.rs:193-204), hash table of T = next_pow2(n) (particle.rs:255).
+ * n must be in 1..FE_MAX_PARTICLES. */
+#define FE_MAX_PARTICLES (1u << 26)
+fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
+                    const float* vel_xyz, int device, fe_ctx** out);
+
+/* Frees everything owned by ctx.  NULL is accepted. */
+fe_status fe_destroy(fe_ctx* ctx);
+
+/* `Resources::sync_with_scene` (src/renderer/resources.rs:85-92): replaces
+ * the parameter block used by later calls. */
+fe_status fe_set_params(fe_ctx* ctx, const fe_params* params);
+fe_status fe_get_params(const fe_ctx* ctx, fe_params* out);
+
+/* `ComputeStep::prepare` for all passes (renderer/mod.rs:137-192): binds
+ * buffers and sizes launches.  Must precede the stage calls and fe_step. */
+fe_status fe_prepare(fe_ctx* ctx);
+
+/* Particle count N and table size T of the context. */
+fe_status fe_get_size(const fe_ctx* ctx, uint32_t* n, uint32_t* table_size);
+
+/* CUDA stream of the context (cudaStream_t as void*). */
+void* fe_get_stream(fe_ctx* ctx);
+
+/* Waits for all work enqueued on the context (the reference's fence wait,
+ * convergence_benchmark.rs:156-162). */
+fe_status fe_synchronize(fe_ctx* ctx);
+
+/* Copies a field between host memory and the context (bytes = element count
+ * of the field × element size, see fe_field).  Enqueued on the context's
+ * stream; download completes before returning. */
+fe_status fe_upload(fe_ctx* ctx, fe_field field, const void* src, size_t bytes);
+fe_status fe_download(fe_ctx* ctx, fe_field field, void* dst, size_t bytes);
+
+/* ------------------------------------------------------------------------- */
+/* Stage entry points: one per `ComputeStep::execute`                         */
+/* ------------------------------------------------------------------------- */
+/* NeighborSearch::execute (neighbor_search.rs:176-231): spatial_hash.comp,
+ * sort (radix or bitonic per params.sort_algorithm), fill(grid_start,
+ * 0xFFFFFFFF), grid_offsets.comp, reorder.comp. */
+fe_status fe_neighbor_search(fe_ctx* ctx);
+/* DensityAlphaPipeline::execute (density_alpha.rs:56-63; density_and_alpha.comp) */
+fe_status fe_density_alpha(fe_ctx* ctx);
+/* ViscosityPipeline::execute (viscosity.rs:56-64; viscosity.comp) */
+fe_status fe_viscosity(fe_ctx* ctx);
+/* DensitySourceTermPipeline::execute (density_source_term.rs:53-62) */
+fe_status fe_density_source(fe_ctx* ctx);
+/* PressureForcePipeline::execute (pressure_force_pipeline.rs:56-64) */
+fe_status fe_pressure_force(fe_ctx* ctx);
+/* PressureUpdatePipeline::execute (pressure_update_pipeline.rs:60-69) */
+fe_status fe_pressure_update(fe_ctx* ctx);
+/* PressureIntegrationPipeline::execute (pressure_integration_pipeline.rs:56-65) */
+fe_status fe_pressure_integration(fe_ctx* ctx);
+/* DivergenceSourceTermPipeline::execute (divergence_source_term.rs:51-60) */
+fe_status fe_divergence_source(fe_ctx* ctx);
+/* DivergenceIntegrationPipeline::execute (divergence_integration.rs:56-64) */
+fe_status fe_divergence_integration(fe_ctx* ctx);
+/* StatsPipeline::execute (stats_pipeline.rs:54-66): fill(0) + stats.comp. */
+fe_status fe_stats_pass(fe_ctx* ctx);
+
+/* Reads the stats of the last stats pass (host read of `stats_buffer`,
+ * renderer/mod.rs:231-236).  Synchronises the context's stream. */
+fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
+
+/* ------------------------------------------------------------------------- */
+/* Whole step                                                                */
+/* ------------------------------------------------------------------------- */
+/* One frame of the physics half of `Renderer::step` (renderer/mod.rs:
+ * 227-342) in the headless form of `submit_substeps`
+ * (convergence_benchmark.rs:108-163):
+ *   [prologue] adaptive CFL dt and early-exit iteration choice from the
+ *              previous frame's stats (mod.rs:231-265), on the device;
+ *   [init]     neighbour search + density/α if FE_STEP_INIT_NS or first call;
+ *   n_substeps × { viscosity, density source, density solve,
+ *                  pressure integration, neighbour search, density/α,
+ *                  divergence source, divergence solve,
+ *                  divergence integration };
+ *   stats.
+ * The frame is replayed from a CUDA graph (conditional WHILE nodes for the
+ * tolerance solver) unless FE_STEP_NO_GRAPH.  `out` may be NULL; when given,
+ * the call synchronises and fills it. */
+fe_status fe_step(fe_ctx* ctx, uint32_t n_substeps, uint32_t flags, fe_stats* out);
+
+/* ------------------------------------------------------------------------- */
+/* Sorting                                                                   */
+/* ------------------------------------------------------------------------- */
+/* Sorts (key, value) pairs by key in device memory, on `stream`
+ * (cudaStream_t as void*, NULL = legacy default stream).  Replaces
+ * `RadixSorter::execute` / `GpuSorter::execute` on an Entry buffer
+ * (sorter.rs:73-115, 325-454).
+ *   FE_SORT_RADIX: stable LSD radix sort, 8-bit digits, the permutation of
+ *     `cpu_radix_sort` (sorter.rs:465-559).  `key_bits` (1..32) bounds the
+ *     key range: keys must be < 2^key_bits; 32 sorts any keys.
+ *   FE_SORT_BITONIC: the compare-exchange network of bitonic_sort.comp;
+ *     n must be a power of two; not stable (same network, same result as
+ *     the reference for the same input).
+ * Scratch is allocated on first use per (device, size class) and kept. */
+fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
+                        uint32_t key_bits, int algorithm, void* stream);
+
+/* Same as fe_sort_pairs with host arrays: copies in, sorts, copies out
+ * (in place). */
+fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* values, uint32_t n,
+                             uint32_t key_bits, int algorithm);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLUID_STEP_H */

@@ -1,0 +1,995 @@
+// fe_oracle.cpp — CPU oracle of the DFSPH step.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for libfluidstep.so, never shipped
+// with it.  Every pass cites the shader it restates (paths are relative to
+// the reference project).  Compile with -ffp-contract=off so that
+// `a * b + c` stays two roundings, as written in the shaders.
+//
+// Semantics decided here (the GLSL leaves them to the driver):
+//   - dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z, left to right;
+//   - length(v) = sqrt(dot(v, v));
+//   - float -> int conversion saturates and maps NaN to 0 (CUDA cvt.rzi);
+//   - GLSL literals without suffix are float (PI = 3.14159274f).
+
+#include "fe_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <type_traits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+
+// ---------------------------------------------------------------------------
+// Small vector type with the shaders' component-wise semantics.
+// ---------------------------------------------------------------------------
+template <class R>
+struct V3 {
+    R x, y, z;
+};
+template <class R>
+struct V4 {
+    R x, y, z, w;
+};
+template <class R>
+inline V3<R> sub(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R>
+inline V3<R> add(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R>
+inline V3<R> scale(R s, V3<R> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class R>
+inline V3<R> scale_r(V3<R> a, R s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class R>
+inline R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R>
+inline V3<R> xyz(const V4<R>& v) { return {v.x, v.y, v.z}; }
+
+template <class R>
+inline int32_t to_int_sat(R v) {
+    if (!(v == v)) return 0;
+    if (v >= R(2147483647.0)) return 2147483647;
+    if (v <= R(-2147483648.0)) return (int32_t)0x80000000u;
+    return (int32_t)v;
+}
+
+// Constants of the shaders as their own type.
+template <class R>
+struct K;
+template <>
+struct K<float> {
+    static float pi() { return 3.1415926535897932384626433832795f; }
+    static float eps_r() { return 1e-6f; }
+};
+template <>
+struct K<double> {
+    static double pi() { return 3.1415926535897932384626433832795; }
+    static double eps_r() { return 1e-6; }
+};
+
+// get_cell_hash (shaders/include/common.glsl:30-35).
+inline uint32_t cell_hash(int32_t cx, int32_t cy, int32_t cz, uint32_t table) {
+    const uint32_t p1 = 73856093u, p2 = 19349663u, p3 = 83492791u;
+    return (((uint32_t)cx * p1) ^ ((uint32_t)cy * p2) ^ ((uint32_t)cz * p3)) % table;
+}
+
+// kernel_w (common.glsl:38-54).
+template <class R>
+inline R kernel_w(R r, R h) {
+    R q = r / h;
+    if (q >= R(1)) return R(0);
+    R h3 = h * h * h;
+    R k = R(8) / (K<R>::pi() * h3);
+    if (q <= R(0.5)) {
+        R q2 = q * q;
+        R q3 = q2 * q;
+        return k * (R(6) * q3 - R(6) * q2 + R(1));
+    } else {
+        R omq = R(1) - q;
+        R omq3 = omq * omq * omq;
+        return k * R(2) * omq3;
+    }
+}
+
+// kernel_grad (common.glsl:56-73), split into the scalar factor
+// grad_factor / (h * r) that multiplies r_vec.
+template <class R>
+inline R kernel_grad_scale(R r, R h) {
+    R q = r / h;
+    if (q >= R(1) || r < K<R>::eps_r()) return R(0);
+    R h3 = h * h * h;
+    R k = R(8) / (K<R>::pi() * h3);
+    R gf;
+    if (q <= R(0.5)) {
+        gf = k * (R(18) * q * q - R(12) * q);
+    } else {
+        R omq = R(1) - q;
+        gf = k * R(-6) * omq * omq;
+    }
+    return gf / (h * r);
+}
+
+int g_threads = 0;  // 0 = OpenMP default
+
+inline int nthreads() {
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-order FP64 sum.  The GPU reduces per-particle doubles in this exact
+// order: chunks of 256 particles (one 256-thread block), inside a chunk a
+// halving tree over each warp of 32 (lane l adds lane l+m, m = 16..1), then a
+// halving tree over the 8 warp sums (m = 4, 2, 1); the chunk sums are added by
+// a single 256-thread block, thread t summing chunks t, t+256, ... in order,
+// followed by the same 256-wide tree.
+// ---------------------------------------------------------------------------
+double tree256(double* a) {  // a[256], destroyed
+    double w[8];
+    for (int wi = 0; wi < 8; ++wi) {
+        double* v = a + 32 * wi;
+        for (int m = 16; m >= 1; m >>= 1)
+            for (int l = 0; l < m; ++l) v[l] = v[l] + v[l + m];
+        w[wi] = v[0];
+    }
+    for (int m = 4; m >= 1; m >>= 1)
+        for (int l = 0; l < m; ++l) w[l] = w[l] + w[l + m];
+    return w[0];
+}
+
+double det_sum(const double* vals, size_t n) {
+    size_t chunks = (n + 255) / 256;
+    std::vector<double> part(chunks);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+    for (long long c = 0; c < (long long)chunks; ++c) {
+        double a[256];
+        for (int t = 0; t < 256; ++t) {
+            size_t i = (size_t)c * 256 + t;
+            a[t] = i < n ? vals[i] : 0.0;
+        }
+        part[c] = tree256(a);
+    }
+    double a[256];
+    for (int t = 0; t < 256; ++t) {
+        double s = 0.0;
+        for (size_t c = t; c < chunks; c += 256) s = s + part[c];
+        a[t] = s;
+    }
+    return tree256(a);
+}
+
+// ---------------------------------------------------------------------------
+// Sorting.
+// ---------------------------------------------------------------------------
+// cpu_radix_sort (src/renderer/pipelines/sorter.rs:465-559).
+void radix_mirror(uint32_t* keys, uint32_t* vals, uint32_t n) {
+    const size_t WG = 256, EPI = 8;
+    size_t num_wg = (n + WG * EPI - 1) / (WG * EPI);
+    std::vector<uint32_t> ak(keys, keys + n), av(vals, vals + n), bk(n), bv(n);
+    for (uint32_t pass = 0; pass < 4; ++pass) {
+        uint32_t shift = pass * 8;
+        bool even = pass % 2 == 0;
+        std::vector<uint32_t>& sk = even ? ak : bk;
+        std::vector<uint32_t>& sv = even ? av : bv;
+        std::vector<uint32_t>& dk = even ? bk : ak;
+        std::vector<uint32_t>& dv = even ? bv : av;
+        std::vector<uint32_t> counts(256 * num_wg, 0);
+        for (size_t wg = 0; wg < num_wg; ++wg) {
+            uint32_t local[256] = {0};
+            for (size_t lid = 0; lid < WG; ++lid) {
+                size_t base = wg * WG * EPI + lid * EPI;
+                for (size_t i = 0; i < EPI; ++i) {
+                    size_t idx = base + i;
+                    if (idx >= n) break;
+                    local[(sk[idx] >> shift) & 0xFF]++;
+                }
+            }
+            for (int d = 0; d < 256; ++d) counts[d * num_wg + wg] = local[d];
+        }
+        uint32_t sums[256];
+        for (size_t lid = 0; lid < 256; ++lid) {
+            uint32_t running = 0;
+            for (size_t i = lid * num_wg; i < lid * num_wg + num_wg; ++i) {
+                uint32_t v = counts[i];
+                counts[i] = running;
+                running += v;
+            }
+            sums[lid] = running;
+        }
+        for (size_t stride = 1; stride < 256; stride *= 2) {
+            uint32_t prev[256];
+            std::memcpy(prev, sums, sizeof(prev));
+            for (size_t lid = stride; lid < 256; ++lid) sums[lid] += prev[lid - stride];
+        }
+        for (size_t lid = 0; lid < 256; ++lid) {
+            uint32_t off = lid == 0 ? 0 : sums[lid - 1];
+            for (size_t i = lid * num_wg; i < lid * num_wg + num_wg; ++i) counts[i] += off;
+        }
+        for (size_t wg = 0; wg < num_wg; ++wg)
+            for (size_t lid = 0; lid < WG; ++lid) {
+                size_t base = wg * WG * EPI + lid * EPI;
+                for (size_t i = 0; i < EPI; ++i) {
+                    size_t idx = base + i;
+                    if (idx >= n) break;
+                    uint32_t d = (sk[idx] >> shift) & 0xFF;
+                    uint32_t dest = counts[d * num_wg + wg]++;
+                    dk[dest] = sk[idx];
+                    dv[dest] = sv[idx];
+                }
+            }
+    }
+    std::memcpy(keys, ak.data(), sizeof(uint32_t) * n);
+    std::memcpy(vals, av.data(), sizeof(uint32_t) * n);
+}
+
+// Parallel stable LSD radix sort (the CPU baseline): per-thread block
+// histograms, a digit-major scan, then a stable scatter per block.
+void radix_parallel(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits) {
+    if (n < 2) return;
+    if (key_bits == 0 || key_bits > 32) key_bits = 32;
+    uint32_t passes = (key_bits + 7) / 8;
+    int T = nthreads();
+    std::vector<uint32_t> tk(n), tv(n);
+    uint32_t* sk = keys;
+    uint32_t* sv = vals;
+    uint32_t* dk = tk.data();
+    uint32_t* dv = tv.data();
+    std::vector<uint32_t> hist((size_t)T * 256);
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        uint32_t shift = pass * 8;
+        std::fill(hist.begin(), hist.end(), 0u);
+#pragma omp parallel num_threads(T)
+        {
+#ifdef _OPENMP
+            int t = omp_get_thread_num();
+#else
+            int t = 0;
+#endif
+            size_t lo = (size_t)n * t / T, hi = (size_t)n * (t + 1) / T;
+            uint32_t* h = hist.data() + (size_t)t * 256;
+            for (size_t i = lo; i < hi; ++i) h[(sk[i] >> shift) & 0xFF]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                uint32_t run = 0;
+                for (int d = 0; d < 256; ++d)
+                    for (int tt = 0; tt < T; ++tt) {
+                        uint32_t c = hist[(size_t)tt * 256 + d];
+                        hist[(size_t)tt * 256 + d] = run;
+                        run += c;
+                    }
+            }
+            for (size_t i = lo; i < hi; ++i) {
+                uint32_t d = (sk[i] >> shift) & 0xFF;
+                uint32_t dest = h[d]++;
+                dk[dest] = sk[i];
+                dv[dest] = sv[i];
+            }
+        }
+        std::swap(sk, dk);
+        std::swap(sv, dv);
+    }
+    if (sk != keys) {
+        std::memcpy(keys, sk, sizeof(uint32_t) * n);
+        std::memcpy(vals, sv, sizeof(uint32_t) * n);
+    }
+}
+
+// bitonic_sort.comp:19-43 driven by GpuSorter::execute (sorter.rs:73-115).
+void bitonic(uint32_t* keys, uint32_t* vals, uint32_t n) {
+    for (uint32_t h = 2; h <= n; h *= 2) {
+        for (uint32_t step = h / 2; step > 0; step /= 2) {
+#pragma omp parallel for schedule(static) num_threads(nthreads()) if (n >= (1u << 16))
+            for (long long ii = 0; ii < (long long)(n / 2); ++ii) {
+                uint32_t i = (uint32_t)ii;
+                uint32_t left = (i / step) * step * 2 + (i % step);
+                uint32_t right = left + step;
+                uint32_t kl = keys[left], kr = keys[right];
+                bool asc = (left & h) == 0u;
+                if ((asc && kl > kr) || (!asc && kl < kr)) {
+                    std::swap(keys[left], keys[right]);
+                    std::swap(vals[left], vals[right]);
+                }
+            }
+        }
+    }
+}
+
+uint32_t next_pow2(uint32_t n) {
+    uint32_t t = 1;
+    while (t < n) t <<= 1;
+    return t;
+}
+
+inline uint32_t fixed_point(float x, float scale) {
+    // min(uint(x * scale), 10000u) of stats.comp:26,29 with a defined result
+    // for NaN (0) and for values beyond the uint range (10000).
+    float v = x * scale;
+    if (!(v > 0.0f)) return 0u;
+    if (v >= 10000.0f) return 10000u;
+    return (uint32_t)v;
+}
+
+// ---------------------------------------------------------------------------
+// The state: GpuPhysicsData (particle.rs:137-161) on the host.
+// ---------------------------------------------------------------------------
+struct Base {
+    virtual ~Base() {}
+    fe_params p{};
+    uint32_t n = 0, T = 0;
+    std::vector<uint32_t> ekey, eidx, grid_start;
+    uint32_t stats[3] = {0, 0, 0};
+    double stats_f64[2] = {0, 0};
+    fe_stats last{};
+    bool initialized = false;
+    // frame-driver state (renderer/mod.rs:231-267)
+    uint32_t iters_rho = 0, iters_div = 0;
+    virtual int neighbor_search() = 0;
+    virtual void density_alpha() = 0;
+    virtual void viscosity() = 0;
+    virtual void density_source() = 0;
+    virtual void pressure_force() = 0;
+    virtual double pressure_update(bool want_residual, bool divergence) = 0;
+    virtual void pressure_integration() = 0;
+    virtual void divergence_source() = 0;
+    virtual void divergence_integration() = 0;
+    virtual void stats_pass() = 0;
+    virtual int download(int field, void* dst, size_t bytes) const = 0;
+    virtual int download_f64(int field, double* dst, size_t count) const = 0;
+    virtual int upload(int field, const void* src, size_t bytes) = 0;
+};
+
+template <class R>
+struct State : Base {
+    std::vector<V4<R>> pos_a, pos_b, vel_a, vel_b, acc;
+    std::vector<R> rho, alpha, src, prs, prs_tmp;
+
+    R h() const { return (R)p.smoothing_radius; }
+    R mass() const { return (R)p.particle_mass; }
+    R dt() const { return (R)p.dt; }
+
+    // Velocity array bound to the divergence passes and stats.
+    std::vector<V4<R>>& vel_div() { return p.mode == FE_MODE_FIXED ? vel_b : vel_a; }
+
+    inline void cell_of(const V4<R>& q, int32_t c[3]) const {
+        R hh = h();
+        c[0] = to_int_sat(std::floor(q.x / hh));
+        c[1] = to_int_sat(std::floor(q.y / hh));
+        c[2] = to_int_sat(std::floor(q.z / hh));
+    }
+
+    // The neighbour walk shared by all particle passes (e.g.
+    // density_and_alpha.comp:31-63): z, y, x offsets; bucket start from
+    // grid_start; walk while the sorted hash matches; skip r2 > h*h.
+    template <class F>
+    inline void for_neighbors(uint32_t i, F&& f) const {
+        const V4<R>& pi = pos_b[i];
+        int32_t c[3];
+        cell_of(pi, c);
+        R hh = h();
+        R h2 = hh * hh;
+        for (int z = -1; z <= 1; ++z)
+            for (int y = -1; y <= 1; ++y)
+                for (int x = -1; x <= 1; ++x) {
+                    uint32_t k = cell_hash((int32_t)((uint32_t)c[0] + (uint32_t)x),
+                                           (int32_t)((uint32_t)c[1] + (uint32_t)y),
+                                           (int32_t)((uint32_t)c[2] + (uint32_t)z), T);
+                    uint32_t s = grid_start[k];
+                    if (s == kEmpty) continue;
+                    for (uint32_t j = s; j < n; ++j) {
+                        if (ekey[j] != k) break;
+                        V3<R> rv = sub(xyz(pi), xyz(pos_b[j]));
+                        R r2 = dot(rv, rv);
+                        if (r2 > h2) continue;
+                        f(j, rv, r2);
+                    }
+                }
+    }
+
+    // NeighborSearch::execute (neighbor_search.rs:176-231).
+    int neighbor_search() override {
+        // spatial_hash.comp:23-36 over T threads.
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)T; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            if (i < n) {
+                int32_t c[3];
+                cell_of(pos_a[i], c);
+                ekey[i] = cell_hash(c[0], c[1], c[2], T);
+                eidx[i] = i;
+            } else {
+                ekey[i] = kEmpty;
+                eidx[i] = kEmpty;
+            }
+        }
+        if (p.sort_algorithm == FE_SORT_RADIX)
+            radix_parallel(ekey.data(), eidx.data(), T, 32);
+        else
+            bitonic(ekey.data(), eidx.data(), T);
+        // fill_buffer(grid_start, 0xFFFFFFFF) + grid_offsets.comp:20-33.
+        std::fill(grid_start.begin(), grid_start.end(), kEmpty);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)T; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            uint32_t key = ekey[i];
+            if (key == kEmpty) continue;
+            uint32_t prev = i == 0 ? kEmpty : ekey[i - 1];
+            if (key != prev) grid_start[key] = i;
+        }
+        // reorder.comp:37-46 (FIXED mode also carries the pressures).
+        bool fixed = p.mode == FE_MODE_FIXED;
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            uint32_t s = eidx[i];
+            pos_b[i] = pos_a[s];
+            vel_b[i] = vel_a[s];
+            if (fixed) prs_tmp[i] = prs[s];
+        }
+        if (fixed) std::swap(prs, prs_tmp);
+        return 0;
+    }
+
+    // density_and_alpha.comp:14-72.
+    void density_alpha() override {
+        R m = mass(), hh = h();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            R density = 0, sum_grad_sq = 0;
+            V3<R> grad_sum{0, 0, 0};
+            for_neighbors(i, [&](uint32_t, V3<R> rv, R r2) {
+                R r = std::sqrt(r2);
+                R w = kernel_w(r, hh);
+                density += m * w;
+                if (r > K<R>::eps_r()) {
+                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                    V3<R> mg = scale(m, grad);
+                    grad_sum = add(grad_sum, mg);
+                    sum_grad_sq += dot(mg, mg);
+                }
+            });
+            rho[i] = density;
+            R a = sum_grad_sq + dot(grad_sum, grad_sum);
+            alpha[i] = a > K<R>::eps_r() ? a : R(0);
+        }
+    }
+
+    // viscosity.comp:17-66: reads velocity_b, writes velocity_a
+    // (viscosity.rs:49-52).
+    void viscosity() override {
+        R m = mass(), hh = h(), nu = (R)p.viscosity, d = dt();
+        V3<R> g{(R)p.gravity[0], (R)p.gravity[1], (R)p.gravity[2]};
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<R> sum{0, 0, 0};
+            V3<R> vi = xyz(vel_b[i]);
+            for_neighbors(i, [&](uint32_t j, V3<R>, R r2) {
+                R r = std::sqrt(r2);
+                R w = kernel_w(r, hh);
+                if (r > K<R>::eps_r()) {
+                    V3<R> vd = sub(xyz(vel_b[j]), vi);
+                    sum = add(sum, scale_r(scale(m / rho[j], vd), w));
+                }
+            });
+            V3<R> vv = add(vi, scale(nu, sum));
+            V3<R> vf = add(vv, scale_r(g, d));
+            vel_a[i] = {vf.x, vf.y, vf.z, R(0)};
+        }
+    }
+
+    // density_source_term.comp:16-74 (velocities = velocity_a,
+    // density_source_term.rs:48).
+    void density_source() override {
+        R m = mass(), hh = h(), d = dt(), rho0 = (R)p.target_density;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<R> vi = xyz(vel_a[i]);
+            R div = 0;
+            for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
+                R r = std::sqrt(r2);
+                if (r > K<R>::eps_r()) {
+                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                    V3<R> vd = sub(vi, xyz(vel_a[j]));
+                    div += m * dot(vd, grad);
+                }
+            });
+            R source = 0;
+            if (d > K<R>::eps_r()) source = ((rho0 - rho[i]) / d) - div;
+            src[i] = source;
+            prs[i] = 0;
+        }
+    }
+
+    // divergence_source_term.comp:14-61 (velocities = velocity_a in
+    // REFERENCE mode, divergence_source_term.rs:47).
+    void divergence_source() override {
+        R m = mass(), hh = h();
+        const std::vector<V4<R>>& vel = vel_div();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<R> vi = xyz(vel[i]);
+            R div = 0;
+            for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
+                R r = std::sqrt(r2);
+                if (r > K<R>::eps_r()) {
+                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                    V3<R> vd = sub(vi, xyz(vel[j]));
+                    div += m * dot(vd, grad);
+                }
+            });
+            src[i] = -div;
+        }
+    }
+
+    // pressure_force.comp:15-78.
+    void pressure_force() override {
+        R m = mass(), hh = h(), eps = K<R>::eps_r();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            R rho_i = rho[i], p_i = prs[i];
+            R p_rho_i = 0;
+            if (rho_i > eps) p_rho_i = p_i / (rho_i * rho_i);
+            V3<R> acc_sum{0, 0, 0};
+            for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
+                R r = std::sqrt(r2);
+                if (r > eps) {
+                    R rho_j = rho[j], p_j = prs[j];
+                    if (rho_j > eps) {
+                        V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                        R p_rho_j = p_j / (rho_j * rho_j);
+                        R term = p_rho_i + p_rho_j;
+                        acc_sum = add(acc_sum, scale(m * term, grad));
+                    }
+                }
+            });
+            acc[i] = {-acc_sum.x, -acc_sum.y, -acc_sum.z, R(0)};
+        }
+    }
+
+    // pressure_update.comp:18-84.  With want_residual, also returns the
+    // fixed-order FP64 sum of the per-particle predicted error of the
+    // pressure *before* this update (tolerance solver, no reference
+    // counterpart): density solve e_i = max(-(dt * (s_i - Ap_i)), 0),
+    // divergence solve e_i = max(-(s_i - Ap_i), 0).
+    std::vector<double> resid;
+    double pressure_update(bool want_residual, bool divergence) override {
+        R m = mass(), hh = h(), d = dt(), omega = (R)p.relax_factor, eps = K<R>::eps_r();
+        if (want_residual) resid.assign(n, 0.0);
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<R> ai = xyz(acc[i]);
+            R alpha_i = alpha[i], rho_i = rho[i], s_i = src[i], p_i = prs[i];
+            R sum_ap = 0;
+            for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
+                R r = std::sqrt(r2);
+                if (r > eps) {
+                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                    V3<R> ad = sub(ai, xyz(acc[j]));
+                    sum_ap += m * dot(ad, grad);
+                }
+            });
+            R ap_i = d * sum_ap;
+            R error = s_i - ap_i;
+            if (alpha_i > eps && rho_i > eps) {
+                R a_ii = -(d / (rho_i * rho_i)) * alpha_i;
+                if (std::fabs(a_ii) > R(1e-20)) {
+                    R corr = (omega * error) / a_ii;
+                    R np = p_i + corr;
+                    prs[i] = np > R(0) ? np : R(0);  // max(x, 0.0), NaN -> 0
+                }
+            }
+            if (want_residual) {
+                R e = divergence ? -error : -(d * error);
+                resid[i] = e > R(0) ? (double)e : 0.0;
+            }
+        }
+        return want_residual ? det_sum(resid.data(), n) : 0.0;
+    }
+
+    // pressure_integration.comp:16-77: reads position_b, writes position_a
+    // and velocity_a in place (pressure_integration_pipeline.rs:49-53).
+    void pressure_integration() override {
+        R d = dt(), r = (R)p.particle_radius;
+        V3<R> mn{(R)p.box_min[0], (R)p.box_min[1], (R)p.box_min[2]};
+        V3<R> mx{(R)p.box_max[0], (R)p.box_max[1], (R)p.box_max[2]};
+        const R rest = R(0.5), fric = R(0.95), e = R(0.001);
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<R> pos = xyz(pos_b[i]);
+            V3<R> vel = xyz(vel_a[i]);
+            V3<R> ap = xyz(acc[i]);
+            V3<R> nv = add(vel, scale_r(ap, d));
+            V3<R> np = add(pos, scale_r(nv, d));
+            if (np.y < mn.y + r) {
+                np.y = mn.y + r + e; nv.y *= -rest; nv.x *= fric; nv.z *= fric;
+            } else if (np.y > mx.y - r) {
+                np.y = mx.y - r - e; nv.y *= -rest; nv.x *= fric; nv.z *= fric;
+            }
+            if (np.x < mn.x + r) {
+                np.x = mn.x + r + e; nv.x *= -rest; nv.y *= fric; nv.z *= fric;
+            } else if (np.x > mx.x - r) {
+                np.x = mx.x - r - e; nv.x *= -rest; nv.y *= fric; nv.z *= fric;
+            }
+            if (np.z < mn.z + r) {
+                np.z = mn.z + r + e; nv.z *= -rest; nv.x *= fric; nv.y *= fric;
+            } else if (np.z > mx.z - r) {
+                np.z = mx.z - r - e; nv.z *= -rest; nv.x *= fric; nv.y *= fric;
+            }
+            pos_a[i] = {np.x, np.y, np.z, R(1)};
+            vel_a[i] = {nv.x, nv.y, nv.z, R(0)};
+        }
+    }
+
+    // divergence_integration.comp:14-43 (velocity part; the colour output is
+    // render-only).
+    void divergence_integration() override {
+        R d = dt();
+        std::vector<V4<R>>& vel = vel_div();
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            V3<R> nv = add(xyz(vel[i]), scale_r(xyz(acc[i]), d));
+            vel[i] = {nv.x, nv.y, nv.z, R(0)};
+        }
+    }
+
+    // StatsPipeline::execute (stats_pipeline.rs:54-66): fill(0) +
+    // stats.comp:18-30, plus FP64 means of |ρ-ρ0| and |s|.
+    void stats_pass() override {
+        const std::vector<V4<R>>& vel = vel_div();
+        uint32_t mx = 0;
+        uint64_t s1 = 0, s2 = 0;
+        std::vector<double> d1(n), d2(n);
+        float rho0f = p.target_density;
+#pragma omp parallel for schedule(static) num_threads(nthreads()) reduction(max : mx) reduction(+ : s1, s2)
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            float vx = (float)vel[i].x, vy = (float)vel[i].y, vz = (float)vel[i].z;
+            float speed = std::sqrt(vx * vx + vy * vy + vz * vz);
+            uint32_t bits;
+            std::memcpy(&bits, &speed, 4);
+            mx = std::max(mx, bits);
+            float de = std::fabs((float)rho[i] - rho0f);
+            s1 += fixed_point(de, 1.0f);
+            float ve = std::fabs((float)src[i]);
+            s2 += fixed_point(ve, 10.0f);
+            d1[i] = std::fabs((double)rho[i] - (double)p.target_density);
+            d2[i] = std::fabs((double)src[i]);
+        }
+        stats[0] = mx;
+        stats[1] = (uint32_t)s1;  // the reference's u32 atomics wrap alike
+        stats[2] = (uint32_t)s2;
+        stats_f64[0] = det_sum(d1.data(), n) / (double)n;
+        stats_f64[1] = det_sum(d2.data(), n) / (double)n;
+    }
+
+    // ---- field transfer --------------------------------------------------
+    const void* field_ptr(int f, size_t& count, int& kind) const {
+        // kind: 0 = R scalar, 1 = V4<R>, 2 = uint32
+        switch (f) {
+            case FE_FIELD_POSITION_A: kind = 1; count = n; return pos_a.data();
+            case FE_FIELD_POSITION_B: kind = 1; count = n; return pos_b.data();
+            case FE_FIELD_VELOCITY_A: kind = 1; count = n; return vel_a.data();
+            case FE_FIELD_VELOCITY_B: kind = 1; count = n; return vel_b.data();
+            case FE_FIELD_DENSITY: kind = 0; count = n; return rho.data();
+            case FE_FIELD_FACTOR: kind = 0; count = n; return alpha.data();
+            case FE_FIELD_SOURCE_TERM: kind = 0; count = n; return src.data();
+            case FE_FIELD_PRESSURE: kind = 0; count = n; return prs.data();
+            case FE_FIELD_PRESSURE_ACCEL: kind = 1; count = n; return acc.data();
+            case FE_FIELD_ENTRY_HASH: kind = 2; count = T; return ekey.data();
+            case FE_FIELD_ENTRY_INDEX: kind = 2; count = T; return eidx.data();
+            case FE_FIELD_GRID_START: kind = 2; count = T; return grid_start.data();
+            case FE_FIELD_STATS: kind = 2; count = 3; return stats;
+        }
+        return nullptr;
+    }
+    int download(int f, void* dst, size_t bytes) const override {
+        size_t count;
+        int kind;
+        const void* src_ptr = field_ptr(f, count, kind);
+        if (!src_ptr || !dst) return FE_ERR_INVALID_ARGUMENT;
+        size_t elems = kind == 1 ? count * 4 : count;
+        if (bytes != elems * 4) return FE_ERR_INVALID_ARGUMENT;
+        if (kind == 2) {
+            std::memcpy(dst, src_ptr, bytes);
+        } else {
+            const R* s = (const R*)src_ptr;
+            float* d = (float*)dst;
+            for (size_t i = 0; i < elems; ++i) d[i] = (float)s[i];
+        }
+        return 0;
+    }
+    int download_f64(int f, double* dst, size_t count_req) const override {
+        size_t count;
+        int kind;
+        const void* src_ptr = field_ptr(f, count, kind);
+        if (!src_ptr || !dst || kind == 2) return FE_ERR_INVALID_ARGUMENT;
+        size_t elems = kind == 1 ? count * 4 : count;
+        if (count_req != elems) return FE_ERR_INVALID_ARGUMENT;
+        const R* s = (const R*)src_ptr;
+        for (size_t i = 0; i < elems; ++i) dst[i] = (double)s[i];
+        return 0;
+    }
+    int upload(int f, const void* src_in, size_t bytes) override {
+        size_t count;
+        int kind;
+        void* dst = const_cast<void*>(field_ptr(f, count, kind));
+        if (!dst || !src_in) return FE_ERR_INVALID_ARGUMENT;
+        size_t elems = kind == 1 ? count * 4 : count;
+        if (bytes != elems * 4) return FE_ERR_INVALID_ARGUMENT;
+        if (kind == 2) {
+            std::memcpy(dst, src_in, bytes);
+        } else {
+            const float* s = (const float*)src_in;
+            R* d = (R*)dst;
+            for (size_t i = 0; i < elems; ++i) d[i] = (R)s[i];
+        }
+        return 0;
+    }
+};
+
+template <class R>
+Base* make_state(const fe_params* params, uint32_t n, const float* pos, const float* vel) {
+    State<R>* s = new (std::nothrow) State<R>();
+    if (!s) return nullptr;
+    s->p = *params;
+    s->n = n;
+    s->T = next_pow2(n);
+    s->pos_a.resize(n);
+    s->pos_b.resize(n);
+    s->vel_a.resize(n);
+    s->vel_b.resize(n);
+    s->acc.assign(n, {0, 0, 0, 0});
+    s->rho.assign(n, 0);
+    s->alpha.assign(n, 0);
+    s->src.assign(n, 0);
+    s->prs.assign(n, 0);
+    s->prs_tmp.assign(n, 0);
+    s->ekey.assign(s->T, 0);
+    s->eidx.assign(s->T, 0);
+    s->grid_start.assign(s->T, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        s->pos_a[i] = {(R)pos[3 * i], (R)pos[3 * i + 1], (R)pos[3 * i + 2], R(1)};
+        s->pos_b[i] = {0, 0, 0, 0};
+        if (vel)
+            s->vel_a[i] = {(R)vel[3 * i], (R)vel[3 * i + 1], (R)vel[3 * i + 2], R(0)};
+        else
+            s->vel_a[i] = {0, 0, 0, 0};
+        s->vel_b[i] = {0, 0, 0, 0};
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Frame driver.
+// ---------------------------------------------------------------------------
+// Prologue of Renderer::step (renderer/mod.rs:231-267): adaptive CFL dt and
+// the early-exit iteration choice, both from the previous frame's stats.
+void frame_prologue(Base* s) {
+    fe_params& p = s->p;
+    float n = (float)s->n;
+    float max_speed;
+    std::memcpy(&max_speed, &s->stats[0], 4);
+    float avg_de = (float)s->stats[1] / (1.0f * n);
+    float avg_ve = (float)s->stats[2] / (10.0f * n);
+    if (p.use_cfl && max_speed > 0.01f) {
+        float h = p.smoothing_radius;
+        float cfl = (p.cfl_lambda * h) / max_speed;
+        // f32::clamp(min, max)
+        if (cfl < p.cfl_min_dt) cfl = p.cfl_min_dt;
+        if (cfl > p.cfl_max_dt) cfl = p.cfl_max_dt;
+        p.dt = std::fmin(cfl, p.dt * p.cfl_growth);
+    }
+    float rho0 = p.target_density;
+    float thr_d = p.density_error_pct / 100.0f * rho0;
+    float thr_v = p.divergence_error_pct / 100.0f * rho0;
+    bool early = p.use_solver_error_threshold && p.solver == FE_SOLVER_FIXED_ITERS;
+    s->iters_rho = (early && avg_de < thr_d) ? 2u : p.density_solver_iterations;
+    s->iters_div = (early && avg_ve < thr_v) ? 1u : p.divergence_solver_iterations;
+}
+
+// The tolerance metric from the residual sum: mean predicted density error
+// over ρ0 (density solve) and mean predicted dρ/dt · dt over ρ0 (divergence
+// solve).  The device computes the same expression in double.
+double solver_metric(Base* s, double sum, bool divergence) {
+    double avg = sum / (double)s->n;
+    if (divergence) avg = avg * (double)s->p.dt;
+    return avg / (double)s->p.target_density;
+}
+
+// One Jacobi solve: fixed count, or the tolerance loop.
+uint32_t solve(Base* s, bool divergence, double* residual_out, bool* cap_hit) {
+    const fe_params& p = s->p;
+    if (p.solver == FE_SOLVER_FIXED_ITERS) {
+        uint32_t k = divergence ? s->iters_div : s->iters_rho;
+        for (uint32_t it = 0; it < k; ++it) {
+            s->pressure_force();
+            s->pressure_update(false, divergence);
+        }
+        *residual_out = 0.0;
+        return k;
+    }
+    double tol = divergence ? (double)p.divergence_tolerance : (double)p.density_tolerance;
+    uint32_t it = 0;
+    double metric = 0.0;
+    for (;;) {
+        s->pressure_force();
+        double sum = s->pressure_update(true, divergence);
+        ++it;
+        metric = solver_metric(s, sum, divergence);
+        if (it >= p.min_iterations && metric <= tol) break;
+        if (it >= p.max_iterations) {
+            *cap_hit = true;
+            break;
+        }
+    }
+    *residual_out = metric;
+    return it;
+}
+
+void substep(Base* s, fe_stats* acc_stats, bool* cap_hit) {
+    double r;
+    s->viscosity();
+    s->density_source();
+    uint32_t kr = solve(s, false, &r, cap_hit);
+    acc_stats->density_iterations = kr;
+    acc_stats->total_density_iterations += kr;
+    acc_stats->density_residual = r;
+    s->pressure_integration();
+    s->neighbor_search();
+    s->density_alpha();
+    s->divergence_source();
+    uint32_t kd = solve(s, true, &r, cap_hit);
+    acc_stats->divergence_iterations = kd;
+    acc_stats->total_divergence_iterations += kd;
+    acc_stats->divergence_residual = r;
+    s->divergence_integration();
+}
+
+void fill_stats(Base* s, fe_stats* out) {
+    out->max_speed_bits = s->stats[0];
+    out->density_error_fp = s->stats[1];
+    out->divergence_error_fp = s->stats[2];
+    std::memcpy(&out->max_speed, &s->stats[0], 4);
+    float n = (float)s->n;
+    out->avg_density_error = (float)s->stats[1] / (1.0f * n);
+    out->avg_divergence_error = (float)s->stats[2] / (10.0f * n);
+    out->avg_density_error_f64 = s->stats_f64[0];
+    out->avg_divergence_error_f64 = s->stats_f64[1];
+    out->dt = s->p.dt;
+}
+
+}  // namespace
+
+struct fo_ctx {
+    Base* s;
+};
+
+extern "C" {
+
+fo_ctx* fo_create(const fe_params* params, uint32_t n, const float* pos_xyz,
+                  const float* vel_xyz, int fp64) {
+    if (!params || !pos_xyz || n == 0 || n > FE_MAX_PARTICLES) return nullptr;
+    fo_ctx* c = new (std::nothrow) fo_ctx;
+    if (!c) return nullptr;
+    c->s = fp64 ? make_state<double>(params, n, pos_xyz, vel_xyz)
+                : make_state<float>(params, n, pos_xyz, vel_xyz);
+    if (!c->s) {
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void fo_destroy(fo_ctx* c) {
+    if (!c) return;
+    delete c->s;
+    delete c;
+}
+
+int fo_set_params(fo_ctx* c, const fe_params* p) {
+    if (!c || !p) return FE_ERR_INVALID_ARGUMENT;
+    c->s->p = *p;
+    return 0;
+}
+int fo_get_params(const fo_ctx* c, fe_params* out) {
+    if (!c || !out) return FE_ERR_INVALID_ARGUMENT;
+    *out = c->s->p;
+    return 0;
+}
+uint32_t fo_table_size(const fo_ctx* c) { return c ? c->s->T : 0; }
+
+int fo_neighbor_search(fo_ctx* c) { return c->s->neighbor_search(); }
+int fo_density_alpha(fo_ctx* c) { c->s->density_alpha(); return 0; }
+int fo_viscosity(fo_ctx* c) { c->s->viscosity(); return 0; }
+int fo_density_source(fo_ctx* c) { c->s->density_source(); return 0; }
+int fo_pressure_force(fo_ctx* c) { c->s->pressure_force(); return 0; }
+int fo_pressure_update(fo_ctx* c) { c->s->pressure_update(false, false); return 0; }
+int fo_pressure_integration(fo_ctx* c) { c->s->pressure_integration(); return 0; }
+int fo_divergence_source(fo_ctx* c) { c->s->divergence_source(); return 0; }
+int fo_divergence_integration(fo_ctx* c) { c->s->divergence_integration(); return 0; }
+int fo_stats_pass(fo_ctx* c) {
+    c->s->stats_pass();
+    fill_stats(c->s, &c->s->last);
+    return 0;
+}
+int fo_read_stats(const fo_ctx* c, fe_stats* out) {
+    if (!c || !out) return FE_ERR_INVALID_ARGUMENT;
+    *out = c->s->last;
+    return 0;
+}
+
+int fo_step(fo_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {
+    if (!c) return FE_ERR_INVALID_ARGUMENT;
+    Base* s = c->s;
+    frame_prologue(s);
+    if ((flags & FE_STEP_INIT_NS) || !s->initialized) {
+        s->neighbor_search();
+        s->density_alpha();
+        s->initialized = true;
+    }
+    fe_stats st = s->last;
+    st.density_iterations = st.divergence_iterations = 0;
+    bool cap_hit = false;
+    for (uint32_t k = 0; k < n_substeps; ++k) substep(s, &st, &cap_hit);
+    s->stats_pass();
+    fill_stats(s, &st);
+    st.substeps = n_substeps;
+    st.flags = cap_hit ? FE_STATS_ITERATION_CAP_HIT : 0u;
+    s->last = st;
+    if (out) *out = st;
+    return 0;
+}
+
+int fo_download(const fo_ctx* c, int field, void* dst, size_t bytes) {
+    if (!c) return FE_ERR_INVALID_ARGUMENT;
+    return c->s->download(field, dst, bytes);
+}
+int fo_download_f64(const fo_ctx* c, int field, double* dst, size_t count) {
+    if (!c) return FE_ERR_INVALID_ARGUMENT;
+    return c->s->download_f64(field, dst, count);
+}
+int fo_upload(fo_ctx* c, int field, const void* src, size_t bytes) {
+    if (!c) return FE_ERR_INVALID_ARGUMENT;
+    return c->s->upload(field, src, bytes);
+}
+
+void fo_sort_radix_mirror(uint32_t* keys, uint32_t* values, uint32_t n) {
+    radix_mirror(keys, values, n);
+}
+void fo_sort_radix_parallel(uint32_t* keys, uint32_t* values, uint32_t n, uint32_t key_bits) {
+    radix_parallel(keys, values, n, key_bits);
+}
+int fo_sort_bitonic(uint32_t* keys, uint32_t* values, uint32_t n) {
+    if (n == 0 || (n & (n - 1))) return FE_ERR_INVALID_ARGUMENT;
+    bitonic(keys, values, n);
+    return 0;
+}
+double fo_det_sum(const double* values, size_t n) { return det_sum(values, n); }
+
+int fo_set_threads(int t) {
+    g_threads = t;
+    return nthreads();
+}
+int fo_get_threads(void) { return nthreads(); }
+
+}  // extern "C"
