@@ -1,0 +1,1060 @@
+// fe_api.cu — host driver and C ABI (include/fluid_step.h).
+//
+// A context is `GpuPhysicsData` + `ComputePipelines` (particle.rs:137-308,
+// pipelines/mod.rs:78-124): it owns the device buffers, a CUDA stream and the
+// recorded frame graphs.  Work is expressed once, through a Recorder that
+// either launches on the stream (stage entry points, FE_STEP_NO_GRAPH) or
+// appends kernel nodes to a CUDA graph — the counterpart of recording into
+// the reference's AutoCommandBufferBuilder and submitting it.  Jacobi loops
+// become conditional WHILE nodes whose condition the pressure-update kernel
+// sets on the device, so a frame with a tolerance-driven solver runs without
+// any host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <tuple>
+#include <utility>
+#include <string>
+#include <vector>
+
+#include "../../include/fluid_step.h"
+#include "fe_device.h"
+#include "fe_kernels.h"
+#include "fe_sort.h"
+
+using namespace fe;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+#define FE_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                      __LINE__);                                                        \
+            return e_ == cudaErrorMemoryAllocation ? FE_ERR_OUT_OF_MEMORY : FE_ERR_CUDA; \
+        }                                                                               \
+    } while (0)
+
+uint32_t next_pow2(uint32_t n) {
+    uint32_t t = 1;
+    while (t < n) t <<= 1;
+    return t;
+}
+
+uint32_t log2_ceil(uint64_t v) {
+    uint32_t b = 0;
+    while ((1ull << b) < v) ++b;
+    return b;
+}
+
+bool finite3(const float* v) {
+    return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
+}
+
+// ---------------------------------------------------------------------------
+// Recorder: eager launches on a stream, or kernel nodes of a graph.
+// ---------------------------------------------------------------------------
+struct Recorder {
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;  // null: eager
+    cudaGraph_t root = nullptr;   // graph owning conditional handles
+    cudaGraphNode_t last = nullptr;
+
+    cudaError_t launch(const void* func, dim3 grid, dim3 block, size_t smem, void** args) {
+        if (!graph) return cudaLaunchKernel(func, grid, block, args, smem, stream);
+        cudaKernelNodeParams p;
+        std::memset(&p, 0, sizeof p);
+        p.func = const_cast<void*>(func);
+        p.gridDim = grid;
+        p.blockDim = block;
+        p.sharedMemBytes = (unsigned)smem;
+        p.kernelParams = args;
+        cudaGraphNode_t node;
+        cudaError_t e = cudaGraphAddKernelNode(&node, graph, last ? &last : nullptr, last ? 1 : 0, &p);
+        if (e == cudaSuccess) last = node;
+        return e;
+    }
+
+    template <typename... KArgs, typename... Args>
+    cudaError_t k(void (*func)(KArgs...), dim3 grid, dim3 block, Args... args) {
+        std::tuple<KArgs...> values(static_cast<KArgs>(args)...);
+        void* ptrs[sizeof...(KArgs) > 0 ? sizeof...(KArgs) : 1];
+        fill_ptrs(values, ptrs, std::index_sequence_for<KArgs...>{});
+        return launch((const void*)func, grid, block, 0, ptrs);
+    }
+
+    template <typename Tuple, size_t... I>
+    static void fill_ptrs(Tuple& t, void** p, std::index_sequence<I...>) {
+        ((p[I] = (void*)&std::get<I>(t)), ...);
+    }
+
+    cudaError_t fill_u32(uint32_t* p, uint32_t v, size_t count) {
+        if (count == 0) return cudaSuccess;
+        size_t blocks = std::min<size_t>((count + 255) / 256, 148 * 8);
+        return k(k_fill_u32, dim3((unsigned)blocks), dim3(256), p, v, count);
+    }
+
+    SortLaunch sort_launch() {
+        SortLaunch L;
+        L.self = this;
+        L.launch_fn = [](void* self, const void* f, dim3 g, dim3 b, size_t smem, void** a) {
+            return static_cast<Recorder*>(self)->launch(f, g, b, smem, a);
+        };
+        L.fill_fn = [](void* self, uint32_t* p, uint32_t v, size_t c) {
+            return static_cast<Recorder*>(self)->fill_u32(p, v, c);
+        };
+        return L;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Parameters
+// ---------------------------------------------------------------------------
+fe_status validate(const fe_params* p) {
+    if (!p) {
+        set_error("params is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    const float scalars[] = {p->particle_radius, p->particle_mass, p->smoothing_radius,
+                             p->target_density, p->viscosity, p->relax_factor, p->dt,
+                             p->density_error_pct, p->divergence_error_pct, p->cfl_lambda,
+                             p->cfl_min_dt, p->cfl_max_dt, p->cfl_growth,
+                             p->density_tolerance, p->divergence_tolerance};
+    for (float v : scalars)
+        if (!std::isfinite(v)) {
+            set_error("non-finite parameter");
+            return FE_ERR_INVALID_ARGUMENT;
+        }
+    if (!finite3(p->gravity) || !finite3(p->box_min) || !finite3(p->box_max)) {
+        set_error("non-finite gravity or box");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (!(p->smoothing_radius > 0.0f)) {
+        set_error("smoothing_radius must be > 0");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (!(p->particle_mass > 0.0f) || !(p->target_density > 0.0f)) {
+        set_error("particle_mass and target_density must be > 0");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (p->dt < 0.0f) {
+        set_error("dt must be >= 0");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    for (int a = 0; a < 3; ++a)
+        if (!(p->box_min[a] < p->box_max[a])) {
+            set_error("box_min must be < box_max on every axis");
+            return FE_ERR_INVALID_ARGUMENT;
+        }
+    if (p->sort_algorithm > FE_SORT_RADIX || p->mode > FE_MODE_FIXED ||
+        p->solver > FE_SOLVER_TOLERANCE || p->warm_start > FE_WARM_LEARNED) {
+        set_error("enum field out of range");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (p->warm_start == FE_WARM_LEARNED) {
+        set_error("learned warm start needs a trained model (not loaded)");
+        return FE_ERR_UNSUPPORTED;
+    }
+    if (p->solver == FE_SOLVER_TOLERANCE &&
+        (p->max_iterations == 0 || p->min_iterations > p->max_iterations)) {
+        set_error("tolerance solver needs 0 < max_iterations and min <= max");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (p->density_solver_iterations > 100000 || p->divergence_solver_iterations > 100000 ||
+        p->max_iterations > 100000) {
+        set_error("iteration counts above 100000");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    for (uint32_t r : p->reserved)
+        if (r) {
+            set_error("reserved fields must be zero");
+            return FE_ERR_INVALID_ARGUMENT;
+        }
+    return FE_OK;
+}
+
+DevParams to_device(const fe_params& p, uint32_t n, uint32_t T, uint32_t table_base,
+                    uint32_t first) {
+    DevParams d;
+    std::memset(&d, 0, sizeof d);
+    d.radius = p.particle_radius;
+    d.mass = p.particle_mass;
+    d.h = p.smoothing_radius;
+    d.rho0 = p.target_density;
+    d.visc = p.viscosity;
+    d.omega = p.relax_factor;
+    d.dt = p.dt;
+    d.gx = p.gravity[0];
+    d.gy = p.gravity[1];
+    d.gz = p.gravity[2];
+    d.bminx = p.box_min[0];
+    d.bminy = p.box_min[1];
+    d.bminz = p.box_min[2];
+    d.bmaxx = p.box_max[0];
+    d.bmaxy = p.box_max[1];
+    d.bmaxz = p.box_max[2];
+    d.n = n;
+    d.T = T;
+    d.table_base = table_base;
+    d.first = first;
+    d.k_rho = p.density_solver_iterations;
+    d.k_div = p.divergence_solver_iterations;
+    d.use_cfl = p.use_cfl;
+    d.use_thr = p.use_solver_error_threshold;
+    d.eta_d_pct = p.density_error_pct;
+    d.eta_v_pct = p.divergence_error_pct;
+    d.cfl_lambda = p.cfl_lambda;
+    d.cfl_min = p.cfl_min_dt;
+    d.cfl_max = p.cfl_max_dt;
+    d.cfl_growth = p.cfl_growth;
+    d.mode = p.mode;
+    d.solver = p.solver;
+    d.tol_d = p.density_tolerance;
+    d.tol_v = p.divergence_tolerance;
+    d.min_it = p.min_iterations;
+    d.max_it = p.max_iterations;
+    d.warm = p.warm_start;
+    return d;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct GraphEntry {
+    uint64_t key;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+};
+
+struct fe_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t n = 0, T = 0;  // particles, table slots (all scenes)
+    std::vector<fe_params> params;  // host copy per scene
+    std::vector<DevParams> dparams;
+    Bufs B;
+    uint32_t* tmp_keys = nullptr;
+    uint32_t* tmp_vals = nullptr;
+    uint32_t* sort_scratch = nullptr;
+    uint4* upart = nullptr;
+    uint32_t key_bits = 32;
+    bool prepared = false;
+    bool initialized = false;
+    std::vector<void*> allocations;
+    std::vector<GraphEntry> graphs;
+    SceneState* h_state = nullptr;   // pinned
+    GlobalState* h_global = nullptr; // pinned
+
+    uint32_t sort_algorithm() const { return params[0].sort_algorithm; }
+    bool fixed_mode() const { return params[0].mode == FE_MODE_FIXED; }
+};
+
+namespace {
+
+template <class T>
+fe_status dev_alloc(fe_ctx* c, T** out, size_t count) {
+    void* p = nullptr;
+    size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return FE_ERR_OUT_OF_MEMORY;
+    }
+    c->allocations.push_back(p);
+    *out = static_cast<T*>(p);
+    return FE_OK;
+}
+
+void release(fe_ctx* c) {
+    if (!c) return;
+    if (c->device >= 0) cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    c->graphs.clear();
+    for (void* p : c->allocations) cudaFree(p);
+    c->allocations.clear();
+    if (c->h_state) cudaFreeHost(c->h_state);
+    if (c->h_global) cudaFreeHost(c->h_global);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+dim3 chunk_grid(const fe_ctx* c) { return dim3(c->B.n_chunks); }
+dim3 flat_grid(uint32_t n) { return dim3((n + kBlock - 1) / kBlock); }
+
+// ---------------------------------------------------------------------------
+// Recording of the passes (shared by the stage calls and the frame graph).
+// ---------------------------------------------------------------------------
+fe_status rec_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return FE_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? FE_ERR_OUT_OF_MEMORY : FE_ERR_CUDA;
+}
+
+#define REC(expr)                                              \
+    do {                                                       \
+        fe_status s_ = rec_check((expr), #expr);               \
+        if (s_ != FE_OK) return s_;                            \
+    } while (0)
+
+// NeighborSearch::execute (neighbor_search.rs:176-231).
+fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
+    Bufs B = c->B;
+    const bool radix = c->sort_algorithm() == FE_SORT_RADIX;
+    uint32_t passes = radix_passes(c->key_bits);
+    // Radix ping-pongs through tmp; hashing into tmp when the pass count is
+    // odd leaves the sorted entries in keys/vals.
+    Bufs H = B;
+    if (radix && (passes % 2 == 1)) {
+        H.keys = c->tmp_keys;
+        H.vals = c->tmp_vals;
+    }
+    REC(R.k(k_hash, chunk_grid(c), dim3(kBlock), H));
+    SortLaunch L = R.sort_launch();
+    if (radix) {
+        bool in_tmp = false;
+        REC(radix_sort(L, H.keys, H.vals, H.keys == B.keys ? c->tmp_keys : B.keys,
+                       H.vals == B.vals ? c->tmp_vals : B.vals, c->n, c->key_bits,
+                       c->sort_scratch, &B.G->flags, &in_tmp));
+    } else {
+        REC(bitonic_sort(L, B.keys, B.vals, c->T));
+    }
+    REC(R.k(k_fill_cells, dim3(std::min<uint32_t>((c->T + 255) / 256, 148 * 8)), dim3(256),
+            B.cells, (size_t)c->T));
+    REC(R.k(k_offsets, flat_grid(c->n), dim3(kBlock), B));
+    REC(R.k(k_reorder, flat_grid(c->n), dim3(kBlock), B, c->fixed_mode() ? 1 : 0));
+    if (c->fixed_mode()) REC(R.k(k_take_pressure, flat_grid(c->n), dim3(kBlock), B));
+    return FE_OK;
+}
+
+fe_status rec_simple(fe_ctx* c, Recorder& R, void (*kern)(Bufs)) {
+    REC(R.k(kern, chunk_grid(c), dim3(kBlock), c->B));
+    return FE_OK;
+}
+
+fe_status rec_stats(fe_ctx* c, Recorder& R) {
+    REC(R.k(k_stats, chunk_grid(c), dim3(kBlock), c->B, c->fixed_mode() ? 1 : 0, c->upart));
+    return FE_OK;
+}
+
+// One Jacobi solve.  Graph: begin kernel, WHILE node {force, update}, end
+// kernel.  Eager: the same kernels with a host loop on the device flag.
+fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
+    Bufs B = c->B;
+    if (!R.graph) {
+        REC(R.k(k_solve_begin, dim3(1), dim3(32), B, which, (cudaGraphConditionalHandle)0, 0));
+        for (uint32_t guard = 0; guard < 200001; ++guard) {
+            uint32_t cond = 0;
+            REC(cudaMemcpyAsync(&cond, &B.G->cond[which], sizeof cond, cudaMemcpyDeviceToHost,
+                                R.stream));
+            REC(cudaStreamSynchronize(R.stream));
+            if (!cond) break;
+            REC(R.k(k_pressure_force, chunk_grid(c), dim3(kBlock), B, which));
+            REC(R.k(k_pressure_update, chunk_grid(c), dim3(kBlock), B, which,
+                    (cudaGraphConditionalHandle)0, 0));
+        }
+        REC(R.k(k_solve_end, dim3(1), dim3(32), B, which));
+        return FE_OK;
+    }
+    cudaGraphConditionalHandle h;
+    REC(cudaGraphConditionalHandleCreate(&h, R.root, 0, 0));
+    REC(R.k(k_solve_begin, dim3(1), dim3(32), B, which, h, 1));
+    // cudaGraphNodeParams has no default constructor (it holds a union);
+    // zeroed storage gives the required all-zero reserved fields.
+    alignas(cudaGraphNodeParams) unsigned char cp_storage[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_storage);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    REC(cudaGraphAddNode(&node, R.graph, R.last ? &R.last : nullptr, R.last ? 1 : 0, &cp));
+    Recorder body;
+    body.stream = R.stream;
+    body.graph = cp.conditional.phGraph_out[0];
+    body.root = R.root;
+    REC(body.k(k_pressure_force, chunk_grid(c), dim3(kBlock), B, which));
+    REC(body.k(k_pressure_update, chunk_grid(c), dim3(kBlock), B, which, h, 1));
+    REC(body.k(k_loop_guard, dim3(1), dim3(32), B, which, h));
+    R.last = node;
+    REC(R.k(k_solve_end, dim3(1), dim3(32), B, which));
+    return FE_OK;
+}
+
+// One substep of Renderer::step (renderer/mod.rs:289-337).
+fe_status rec_substep(fe_ctx* c, Recorder& R) {
+    Bufs B = c->B;
+    const int fixed = c->fixed_mode() ? 1 : 0;
+    fe_status s;
+    if ((s = rec_simple(c, R, k_viscosity))) return s;
+    if ((s = rec_simple(c, R, k_density_source))) return s;
+    if ((s = rec_solve(c, R, 0))) return s;
+    if ((s = rec_simple(c, R, k_pressure_integration))) return s;
+    if ((s = rec_neighbor_search(c, R))) return s;
+    if ((s = rec_simple(c, R, k_density_alpha))) return s;
+    REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));
+    if ((s = rec_solve(c, R, 1))) return s;
+    REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), B, fixed));
+    REC(R.k(k_count_substep, dim3(1), dim3(64), B));
+    return FE_OK;
+}
+
+fe_status rec_frame(fe_ctx* c, Recorder& R, uint32_t n_substeps, bool init) {
+    fe_status s;
+    REC(R.k(k_frame_prologue, dim3(1), dim3(64), c->B));
+    if (init) {
+        if ((s = rec_neighbor_search(c, R))) return s;
+        if ((s = rec_simple(c, R, k_density_alpha))) return s;
+    }
+    for (uint32_t k = 0; k < n_substeps; ++k)
+        if ((s = rec_substep(c, R))) return s;
+    return rec_stats(c, R);
+}
+
+fe_status need_prepared(fe_ctx* c, const char* what) {
+    if (!c) {
+        set_error("%s: context is NULL", what);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (!c->prepared) {
+        set_error("%s: call prepare() before execute()", what);
+        return FE_ERR_NOT_PREPARED;
+    }
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        set_error("%s: cudaSetDevice failed", what);
+        return FE_ERR_CUDA;
+    }
+    return FE_OK;
+}
+
+Recorder eager(fe_ctx* c) {
+    Recorder R;
+    R.stream = c->stream;
+    return R;
+}
+
+fe_status upload_params(fe_ctx* c) {
+    FE_CUDA(cudaMemcpyAsync(c->B.P, c->dparams.data(), sizeof(DevParams) * c->dparams.size(),
+                            cudaMemcpyHostToDevice, c->stream));
+    return FE_OK;
+}
+
+fe_status run_refresh_pr(fe_ctx* c) {
+    Recorder R = eager(c);
+    REC(R.k(k_refresh_pr, flat_grid(c->n), dim3(kBlock), c->B));
+    return FE_OK;
+}
+
+size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem) {
+    switch (f) {
+        case FE_FIELD_POSITION_A: *dptr = c->B.pos_a; *elem = 16; return (size_t)c->n * 16;
+        case FE_FIELD_POSITION_B: *dptr = c->B.pos_b; *elem = 16; return (size_t)c->n * 16;
+        case FE_FIELD_VELOCITY_A: *dptr = c->B.vel_a; *elem = 16; return (size_t)c->n * 16;
+        case FE_FIELD_VELOCITY_B: *dptr = c->B.vel_b; *elem = 16; return (size_t)c->n * 16;
+        case FE_FIELD_DENSITY: *dptr = c->B.rho; *elem = 4; return (size_t)c->n * 4;
+        case FE_FIELD_FACTOR: *dptr = c->B.alpha; *elem = 4; return (size_t)c->n * 4;
+        case FE_FIELD_SOURCE_TERM: *dptr = c->B.src; *elem = 4; return (size_t)c->n * 4;
+        case FE_FIELD_PRESSURE: *dptr = c->B.prs; *elem = 4; return (size_t)c->n * 4;
+        case FE_FIELD_PRESSURE_ACCEL: *dptr = c->B.acc; *elem = 16; return (size_t)c->n * 16;
+        case FE_FIELD_ENTRY_HASH: *dptr = c->B.keys; *elem = 4; return (size_t)c->T * 4;
+        case FE_FIELD_ENTRY_INDEX: *dptr = c->B.vals; *elem = 4; return (size_t)c->T * 4;
+        case FE_FIELD_GRID_START: *dptr = c->B.cells; *elem = 8; return (size_t)c->T * 4;
+        case FE_FIELD_STATS: *dptr = c->B.S; *elem = 4; return 12;
+        default: return 0;
+    }
+}
+
+uint64_t graph_key(const fe_ctx* c, uint32_t n_substeps, bool init) {
+    return (uint64_t)n_substeps | ((uint64_t)init << 32) | ((uint64_t)c->sort_algorithm() << 33) |
+           ((uint64_t)c->fixed_mode() << 34);
+}
+
+fe_status get_graph(fe_ctx* c, uint32_t n_substeps, bool init, cudaGraphExec_t* out) {
+    uint64_t key = graph_key(c, n_substeps, init);
+    for (auto& g : c->graphs)
+        if (g.key == key) {
+            *out = g.exec;
+            return FE_OK;
+        }
+    GraphEntry g{key, nullptr, nullptr};
+    FE_CUDA(cudaGraphCreate(&g.graph, 0));
+    Recorder R;
+    R.stream = c->stream;
+    R.graph = g.graph;
+    R.root = g.graph;
+    fe_status s = rec_frame(c, R, n_substeps, init);
+    if (s != FE_OK) {
+        cudaGraphDestroy(g.graph);
+        return s;
+    }
+    cudaError_t e = cudaGraphInstantiate(&g.exec, g.graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g.graph);
+        set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e));
+        return FE_ERR_CUDA;
+    }
+    if (c->graphs.size() >= 8) {
+        cudaStreamSynchronize(c->stream);
+        cudaGraphExecDestroy(c->graphs.front().exec);
+        cudaGraphDestroy(c->graphs.front().graph);
+        c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back(g);
+    *out = g.exec;
+    return FE_OK;
+}
+
+fe_status collect_stats(fe_ctx* c, fe_stats* out) {
+    FE_CUDA(cudaMemcpyAsync(c->h_state, c->B.S, sizeof(SceneState), cudaMemcpyDeviceToHost,
+                            c->stream));
+    FE_CUDA(cudaMemcpyAsync(c->h_global, c->B.G, sizeof(GlobalState), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DevParams dp;
+    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    const SceneState& S = *c->h_state;
+    std::memset(out, 0, sizeof *out);
+    out->max_speed_bits = S.stats[0];
+    out->density_error_fp = S.stats[1];
+    out->divergence_error_fp = S.stats[2];
+    std::memcpy(&out->max_speed, &S.stats[0], 4);
+    float n = (float)dp.n;
+    out->avg_density_error = (float)S.stats[1] / (1.0f * n);
+    out->avg_divergence_error = (float)S.stats[2] / (10.0f * n);
+    out->dt = dp.dt;
+    out->avg_density_error_f64 = S.stats_f64[0];
+    out->avg_divergence_error_f64 = S.stats_f64[1];
+    out->density_residual = S.last_metric[0];
+    out->divergence_residual = S.last_metric[1];
+    out->density_iterations = S.last_iters[0];
+    out->divergence_iterations = S.last_iters[1];
+    out->total_density_iterations = S.total_iters[0];
+    out->total_divergence_iterations = S.total_iters[1];
+    out->substeps = S.substeps;
+    uint32_t flags = c->h_global->flags;
+    if (S.nonfinite) flags |= 0x8u;
+    out->flags = flags;
+    // host-side mirror of the device dt
+    c->params[0].dt = dp.dt;
+    return FE_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+uint32_t fe_abi_version(void) { return FE_ABI_VERSION; }
+
+const char* fe_status_string(fe_status s) {
+    switch (s) {
+        case FE_OK: return "FE_OK";
+        case FE_ERR_INVALID_ARGUMENT: return "FE_ERR_INVALID_ARGUMENT";
+        case FE_ERR_NOT_PREPARED: return "FE_ERR_NOT_PREPARED";
+        case FE_ERR_CUDA: return "FE_ERR_CUDA";
+        case FE_ERR_OUT_OF_MEMORY: return "FE_ERR_OUT_OF_MEMORY";
+        case FE_ERR_NON_FINITE: return "FE_ERR_NON_FINITE";
+        case FE_ERR_ITERATION_CAP: return "FE_ERR_ITERATION_CAP";
+        case FE_ERR_TIMEOUT: return "FE_ERR_TIMEOUT";
+        case FE_ERR_NO_DEVICE: return "FE_ERR_NO_DEVICE";
+        case FE_ERR_CAPACITY: return "FE_ERR_CAPACITY";
+        case FE_ERR_UNSUPPORTED: return "FE_ERR_UNSUPPORTED";
+    }
+    return "FE_ERR_UNKNOWN";
+}
+
+const char* fe_last_error(void) { return g_last_error.c_str(); }
+
+void fe_default_params(fe_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    const float radius = 0.020f;
+    const float spacing = radius * 2.0f;
+    p->particle_radius = radius;
+    p->particle_mass = 1000.0f * (spacing * spacing * spacing);
+    p->smoothing_radius = radius * 4.0f;
+    p->target_density = 1000.0f;
+    p->viscosity = 0.15f;
+    p->relax_factor = 0.5f;
+    p->dt = 0.005f;
+    p->density_solver_iterations = 4;
+    p->divergence_solver_iterations = 4;
+    p->gravity[1] = -9.81f;
+    p->box_min[0] = -1.5f;
+    p->box_min[1] = 0.0f;
+    p->box_min[2] = -1.0f;
+    p->box_max[0] = 0.8f;
+    p->box_max[1] = 4.0f;
+    p->box_max[2] = 1.0f;
+    p->grid_res[0] = p->grid_res[1] = p->grid_res[2] = 128;
+    p->sort_algorithm = FE_SORT_RADIX;
+    p->density_error_pct = 0.1f;
+    p->divergence_error_pct = 0.5f;
+    p->cfl_lambda = 0.4f;
+    p->cfl_min_dt = 0.001f;
+    p->cfl_max_dt = 0.05f;
+    p->cfl_growth = 1.1f;
+    p->mode = FE_MODE_REFERENCE;
+    p->solver = FE_SOLVER_FIXED_ITERS;
+    p->density_tolerance = 0.001f;
+    p->divergence_tolerance = 0.001f;
+    p->min_iterations = 2;
+    p->max_iterations = 100;
+    p->warm_start = FE_WARM_REFERENCE;
+}
+
+fe_status fe_validate_params(const fe_params* p) { return validate(p); }
+
+fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
+                    const float* vel_xyz, int device, fe_ctx** out) {
+    if (!out) {
+        set_error("out is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    fe_status s = validate(params);
+    if (s != FE_OK) return s;
+    if (n == 0 || n > FE_MAX_PARTICLES) {
+        set_error("particle count %u outside 1..%u", n, FE_MAX_PARTICLES);
+        return n == 0 ? FE_ERR_INVALID_ARGUMENT : FE_ERR_CAPACITY;
+    }
+    if (!pos_xyz) {
+        set_error("pos_xyz is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    for (size_t i = 0; i < (size_t)n * 3; ++i)
+        if (!std::isfinite(pos_xyz[i]) || (vel_xyz && !std::isfinite(vel_xyz[i]))) {
+            set_error("non-finite position or velocity at particle %zu", i / 3);
+            return FE_ERR_NON_FINITE;
+        }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        set_error("no CUDA device %d", device);
+        return FE_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        set_error("device %d is not sm_100 (Blackwell)", device);
+        return FE_ERR_NO_DEVICE;
+    }
+    FE_CUDA(cudaSetDevice(device));
+    fe_ctx* c = new fe_ctx();
+    c->device = device;
+    c->n = n;
+    c->T = next_pow2(n);
+    c->key_bits = log2_ceil(c->T);
+    if (c->key_bits == 0) c->key_bits = 1;
+    c->params.assign(1, *params);
+    c->dparams.assign(1, to_device(*params, n, c->T, 0, 0));
+    auto fail = [&](fe_status st) {
+        release(c);
+        delete c;
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("cudaStreamCreate failed");
+        return fail(FE_ERR_CUDA);
+    }
+    Bufs& B = c->B;
+    std::memset(&B, 0, sizeof B);
+    const uint32_t nchunks = (n + kBlock - 1) / kBlock;
+    B.n_total = n;
+    B.T_total = c->T;
+    B.n_chunks = nchunks;
+    B.n_scenes = 1;
+    uint4* chunks_d = nullptr;
+    const size_t scratch_words = radix_scratch_words(n, c->key_bits);
+    if ((s = dev_alloc(c, &B.pos_a, n)) || (s = dev_alloc(c, &B.pos_b, n)) ||
+        (s = dev_alloc(c, &B.vel_a, n)) || (s = dev_alloc(c, &B.vel_b, n)) ||
+        (s = dev_alloc(c, &B.acc, n)) || (s = dev_alloc(c, &B.rho, n)) ||
+        (s = dev_alloc(c, &B.alpha, n)) || (s = dev_alloc(c, &B.src, n)) ||
+        (s = dev_alloc(c, &B.prs, n)) || (s = dev_alloc(c, &B.prs_tmp, n)) ||
+        (s = dev_alloc(c, &B.pr, n)) || (s = dev_alloc(c, &B.keys, c->T)) ||
+        (s = dev_alloc(c, &B.vals, c->T)) || (s = dev_alloc(c, &B.cells, c->T)) ||
+        (s = dev_alloc(c, &B.nbr_count, n)) || (s = dev_alloc(c, &B.nbr, (size_t)kNbrCap * n)) ||
+        (s = dev_alloc(c, &chunks_d, nchunks)) || (s = dev_alloc(c, &B.P, 1)) ||
+        (s = dev_alloc(c, &B.S, 1)) || (s = dev_alloc(c, &B.G, 1)) ||
+        (s = dev_alloc(c, &B.partials, 2 * (size_t)nchunks)) ||
+        (s = dev_alloc(c, &c->upart, nchunks)) || (s = dev_alloc(c, &c->tmp_keys, n)) ||
+        (s = dev_alloc(c, &c->tmp_vals, n)) ||
+        (s = dev_alloc(c, &c->sort_scratch, scratch_words)))
+        return fail(s);
+    B.chunks = chunks_d;
+    if (cudaMallocHost(&c->h_state, sizeof(SceneState)) != cudaSuccess ||
+        cudaMallocHost(&c->h_global, sizeof(GlobalState)) != cudaSuccess) {
+        set_error("cudaMallocHost failed");
+        return fail(FE_ERR_OUT_OF_MEMORY);
+    }
+    // Initial state (GpuPhysicsData::new): positions w = 1, velocities 0.
+    std::vector<float4> h4(n);
+    for (uint32_t i = 0; i < n; ++i)
+        h4[i] = make_float4(pos_xyz[3 * i], pos_xyz[3 * i + 1], pos_xyz[3 * i + 2], 1.0f);
+    std::vector<uint4> hc(nchunks);
+    for (uint32_t k = 0; k < nchunks; ++k)
+        hc[k] = make_uint4(k * kBlock, std::min<uint32_t>(kBlock, n - k * kBlock), 0, k);
+    auto setup = [&]() -> fe_status {
+        FE_CUDA(cudaMemcpy(B.pos_a, h4.data(), (size_t)n * 16, cudaMemcpyHostToDevice));
+        for (uint32_t i = 0; i < n; ++i)
+            h4[i] = vel_xyz ? make_float4(vel_xyz[3 * i], vel_xyz[3 * i + 1], vel_xyz[3 * i + 2], 0.0f)
+                            : make_float4(0, 0, 0, 0);
+        FE_CUDA(cudaMemcpy(B.vel_a, h4.data(), (size_t)n * 16, cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(chunks_d, hc.data(), sizeof(uint4) * nchunks, cudaMemcpyHostToDevice));
+        for (void* p : {(void*)B.pos_b, (void*)B.vel_b, (void*)B.acc})
+            FE_CUDA(cudaMemset(p, 0, (size_t)n * 16));
+        for (void* p : {(void*)B.rho, (void*)B.alpha, (void*)B.src, (void*)B.prs,
+                        (void*)B.prs_tmp, (void*)B.nbr_count})
+            FE_CUDA(cudaMemset(p, 0, (size_t)n * 4));
+        FE_CUDA(cudaMemset(B.keys, 0, (size_t)n * 4));
+        FE_CUDA(cudaMemset(B.vals, 0, (size_t)n * 4));
+        if (c->T > n) {  // sentinel tail of grid_entries (spatial_hash.comp:33-35)
+            FE_CUDA(cudaMemset(B.keys + n, 0xFF, (size_t)(c->T - n) * 4));
+            FE_CUDA(cudaMemset(B.vals + n, 0xFF, (size_t)(c->T - n) * 4));
+        }
+        FE_CUDA(cudaMemset(B.cells, 0xFF, (size_t)c->T * 8));
+        FE_CUDA(cudaMemset(B.S, 0, sizeof(SceneState)));
+        FE_CUDA(cudaMemset(B.G, 0, sizeof(GlobalState)));
+        FE_CUDA(cudaMemcpy(B.P, c->dparams.data(), sizeof(DevParams), cudaMemcpyHostToDevice));
+        fe_status st = run_refresh_pr(c);
+        if (st != FE_OK) return st;
+        FE_CUDA(cudaStreamSynchronize(c->stream));
+        return FE_OK;
+    };
+    if ((s = setup()) != FE_OK) return fail(s);
+    *out = c;
+    return FE_OK;
+}
+
+fe_status fe_destroy(fe_ctx* c) {
+    if (!c) return FE_OK;
+    release(c);
+    delete c;
+    return FE_OK;
+}
+
+fe_status fe_set_params(fe_ctx* c, const fe_params* p) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    fe_status s = validate(p);
+    if (s != FE_OK) return s;
+    if (p->sort_algorithm == FE_SORT_BITONIC && c->B.n_scenes > 1) {
+        set_error("bitonic sort is single-scene only");
+        return FE_ERR_UNSUPPORTED;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    c->params[0] = *p;
+    const DevParams& old = c->dparams[0];
+    c->dparams[0] = to_device(*p, old.n, old.T, old.table_base, old.first);
+    return upload_params(c);
+}
+
+fe_status fe_get_params(const fe_ctx* c, fe_params* out) {
+    if (!c || !out) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    fe_ctx* m = const_cast<fe_ctx*>(c);
+    FE_CUDA(cudaSetDevice(c->device));
+    DevParams dp;
+    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    m->params[0].dt = dp.dt;
+    *out = c->params[0];
+    return FE_OK;
+}
+
+fe_status fe_prepare(fe_ctx* c) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    c->prepared = true;
+    return FE_OK;
+}
+
+fe_status fe_get_size(const fe_ctx* c, uint32_t* n, uint32_t* t) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (n) *n = c->n;
+    if (t) *t = c->T;
+    return FE_OK;
+}
+
+void* fe_get_stream(fe_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+fe_status fe_synchronize(fe_ctx* c) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    return FE_OK;
+}
+
+fe_status fe_upload(fe_ctx* c, fe_field f, const void* src, size_t bytes) {
+    if (!c || !src) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    void* d;
+    size_t elem;
+    size_t need = field_bytes(c, f, &d, &elem);
+    if (need == 0 || bytes != need || f == FE_FIELD_STATS || f == FE_FIELD_GRID_START) {
+        set_error("field %d: expected %zu bytes, got %zu (or read-only field)", (int)f, need, bytes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    FE_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY) return run_refresh_pr(c);
+    return FE_OK;
+}
+
+fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
+    if (!c || !dst) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    void* d;
+    size_t elem;
+    size_t need = field_bytes(c, f, &d, &elem);
+    if (need == 0 || bytes != need) {
+        set_error("field %d: expected %zu bytes, got %zu", (int)f, need, bytes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    if (f == FE_FIELD_GRID_START) {
+        FE_CUDA(cudaMemcpy2DAsync(dst, 4, d, 8, 4, c->T, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        FE_CUDA(cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    return FE_OK;
+}
+
+#define FE_STAGE(name, body)                                 \
+    fe_status name(fe_ctx* c) {                              \
+        fe_status s_ = need_prepared(c, #name);              \
+        if (s_ != FE_OK) return s_;                          \
+        Recorder R = eager(c);                               \
+        body;                                                \
+    }
+
+FE_STAGE(fe_neighbor_search, return rec_neighbor_search(c, R))
+FE_STAGE(fe_density_alpha, return rec_simple(c, R, k_density_alpha))
+FE_STAGE(fe_viscosity, return rec_simple(c, R, k_viscosity))
+FE_STAGE(fe_density_source, return rec_simple(c, R, k_density_source))
+FE_STAGE(fe_pressure_force, REC(R.k(k_pressure_force, chunk_grid(c), dim3(kBlock), c->B, -1));
+         return FE_OK)
+FE_STAGE(fe_pressure_update,
+         REC(R.k(k_pressure_update, chunk_grid(c), dim3(kBlock), c->B, -1,
+                 (cudaGraphConditionalHandle)0, 0));
+         return FE_OK)
+FE_STAGE(fe_pressure_integration, return rec_simple(c, R, k_pressure_integration))
+FE_STAGE(fe_divergence_source,
+         REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), c->B, c->fixed_mode() ? 1 : 0));
+         return FE_OK)
+FE_STAGE(fe_divergence_integration,
+         REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), c->B,
+                 c->fixed_mode() ? 1 : 0));
+         return FE_OK)
+FE_STAGE(fe_stats_pass, return rec_stats(c, R))
+
+fe_status fe_read_stats(fe_ctx* c, fe_stats* out) {
+    if (!c || !out) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    return collect_stats(c, out);
+}
+
+fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {
+    fe_status s = need_prepared(c, "fe_step");
+    if (s != FE_OK) return s;
+    if (n_substeps > 1024) {
+        set_error("n_substeps %u above 1024", n_substeps);
+        return FE_ERR_CAPACITY;
+    }
+    const bool init = (flags & FE_STEP_INIT_NS) || !c->initialized;
+    if (flags & FE_STEP_NO_GRAPH) {
+        Recorder R = eager(c);
+        s = rec_frame(c, R, n_substeps, init);
+        if (s != FE_OK) return s;
+    } else {
+        cudaGraphExec_t exec;
+        s = get_graph(c, n_substeps, init, &exec);
+        if (s != FE_OK) return s;
+        FE_CUDA(cudaGraphLaunch(exec, c->stream));
+    }
+    c->initialized = true;
+    if (!out) return FE_OK;
+    s = collect_stats(c, out);
+    if (s != FE_OK) return s;
+    if (out->flags & 0x4u) {
+        set_error("a bounded device wait timed out (look-back)");
+        return FE_ERR_TIMEOUT;
+    }
+    if (out->flags & 0x8u) {
+        set_error("non-finite velocity, density or source term in the stats pass");
+        return FE_ERR_NON_FINITE;
+    }
+    return FE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Standalone sort (device buffers).  Scratch per device, grown on demand;
+// an event serialises users of the same scratch across streams.
+// ---------------------------------------------------------------------------
+namespace {
+struct SortScratch {
+    int device = -1;
+    uint32_t cap = 0;
+    uint32_t* tk = nullptr;
+    uint32_t* tv = nullptr;
+    uint32_t* words = nullptr;
+    size_t nwords = 0;
+    uint32_t* flags = nullptr;
+    cudaEvent_t done = nullptr;
+};
+std::mutex g_sort_mutex;
+SortScratch g_sort[16];
+}  // namespace
+
+fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
+                        int algorithm, void* stream_ptr) {
+    if ((!keys || !vals) && n > 0) {
+        set_error("NULL keys or values");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (algorithm != FE_SORT_RADIX && algorithm != FE_SORT_BITONIC) {
+        set_error("unknown sort algorithm %d", algorithm);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (key_bits > 32) {
+        set_error("key_bits %u above 32", key_bits);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (n > FE_MAX_PARTICLES) {
+        set_error("n %u above %u", n, FE_MAX_PARTICLES);
+        return FE_ERR_CAPACITY;
+    }
+    if (n < 2) return FE_OK;
+    if (algorithm == FE_SORT_BITONIC && (n & (n - 1))) {
+        set_error("bitonic sort needs a power-of-two length (sorter.rs:57-60)");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    Recorder R;
+    R.stream = stream;
+    SortLaunch L = R.sort_launch();
+    if (algorithm == FE_SORT_BITONIC) {
+        REC(bitonic_sort(L, keys, vals, n));
+        return FE_OK;
+    }
+    int dev;
+    FE_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) {
+        set_error("device index %d unsupported", dev);
+        return FE_ERR_NO_DEVICE;
+    }
+    std::lock_guard<std::mutex> lock(g_sort_mutex);
+    SortScratch& S = g_sort[dev];
+    size_t words = radix_scratch_words(n, key_bits ? key_bits : 32);
+    if (S.cap < n || S.nwords < words) {
+        if (S.done) FE_CUDA(cudaEventSynchronize(S.done));
+        cudaFree(S.tk);
+        cudaFree(S.tv);
+        cudaFree(S.words);
+        S.tk = S.tv = S.words = nullptr;
+        uint32_t cap = std::max(n, S.cap);
+        size_t nw = std::max(words, S.nwords);
+        FE_CUDA(cudaMalloc(&S.tk, (size_t)cap * 4));
+        FE_CUDA(cudaMalloc(&S.tv, (size_t)cap * 4));
+        FE_CUDA(cudaMalloc(&S.words, (nw + 8) * 4));
+        S.cap = cap;
+        S.nwords = nw;
+        S.flags = S.words + nw;
+        FE_CUDA(cudaMemset(S.flags, 0, 32));
+        if (!S.done) FE_CUDA(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+        S.device = dev;
+    } else {
+        FE_CUDA(cudaStreamWaitEvent(stream, S.done, 0));
+    }
+    bool in_tmp = false;
+    REC(radix_sort(L, keys, vals, S.tk, S.tv, n, key_bits ? key_bits : 32, S.words, S.flags,
+                   &in_tmp));
+    if (in_tmp) {
+        FE_CUDA(cudaMemcpyAsync(keys, S.tk, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream));
+        FE_CUDA(cudaMemcpyAsync(vals, S.tv, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream));
+    }
+    FE_CUDA(cudaEventRecord(S.done, stream));
+    return FE_OK;
+}
+
+fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
+                             int algorithm) {
+    if ((!keys || !vals) && n > 0) {
+        set_error("NULL keys or values");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (n < 2) return FE_OK;
+    uint32_t *dk = nullptr, *dv = nullptr;
+    FE_CUDA(cudaMalloc(&dk, (size_t)n * 4));
+    if (cudaMalloc(&dv, (size_t)n * 4) != cudaSuccess) {
+        cudaFree(dk);
+        set_error("cudaMalloc failed");
+        return FE_ERR_OUT_OF_MEMORY;
+    }
+    fe_status s = FE_OK;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMemcpyAsync(dk, keys, (size_t)n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(dv, vals, (size_t)n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        set_error("host-to-device copy failed");
+        s = FE_ERR_CUDA;
+    }
+    if (s == FE_OK) s = fe_sort_pairs(dk, dv, n, key_bits, algorithm, st);
+    if (s == FE_OK &&
+        (cudaMemcpyAsync(keys, dk, (size_t)n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+         cudaMemcpyAsync(vals, dv, (size_t)n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+         cudaStreamSynchronize(st) != cudaSuccess)) {
+        set_error("device-to-host copy failed");
+        s = FE_ERR_CUDA;
+    }
+    if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    cudaFree(dk);
+    cudaFree(dv);
+    return s;
+}
+
+}  // extern "C"

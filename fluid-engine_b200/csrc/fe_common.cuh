@@ -1,0 +1,129 @@
+// fe_common.cuh — device helpers shared by the DFSPH kernels.
+//
+// Numerics: this library is compiled with -fmad=false -prec-div=true
+// -prec-sqrt=true -ftz=false, so every expression below rounds exactly as the
+// host oracle does (IEEE single precision, one rounding per operation, in
+// source order).  The shader formulas are restated from
+// shaders/include/common.glsl.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fe_device.h"
+
+namespace fe {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+// GLSL `PI` of common.glsl:4 as a float literal.
+constexpr float kPi = 3.1415926535897932384626433832795f;
+constexpr float kEpsR = 1e-6f;
+
+struct f3 {
+    float x, y, z;
+};
+__device__ __forceinline__ f3 xyz(float4 v) { return {v.x, v.y, v.z}; }
+__device__ __forceinline__ f3 sub(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 add(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 scale(float s, f3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ f3 scale_r(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+// dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z, as the oracle defines it.
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// get_cell_hash (common.glsl:30-35).
+__device__ __forceinline__ uint32_t cell_hash(int cx, int cy, int cz, uint32_t table) {
+    return (((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u) ^
+            ((uint32_t)cz * 83492791u)) % table;
+}
+
+// ivec3(floor(p / h)): IEEE division, floor, saturating conversion (NaN -> 0).
+__device__ __forceinline__ int cell_coord(float p, float h) {
+    return __float2int_rz(floorf(p / h));
+}
+
+// kernel_w (common.glsl:38-54).
+__device__ __forceinline__ float kernel_w(float r, float h) {
+    float q = r / h;
+    if (q >= 1.0f) return 0.0f;
+    float h3 = h * h * h;
+    float k = 8.0f / (kPi * h3);
+    if (q <= 0.5f) {
+        float q2 = q * q;
+        float q3 = q2 * q;
+        return k * (6.0f * q3 - 6.0f * q2 + 1.0f);
+    } else {
+        float omq = 1.0f - q;
+        float omq3 = omq * omq * omq;
+        return k * 2.0f * omq3;
+    }
+}
+
+// kernel_grad (common.glsl:56-73) as the scalar that multiplies r_vec.
+__device__ __forceinline__ float kernel_grad_scale(float r, float h) {
+    float q = r / h;
+    if (q >= 1.0f || r < kEpsR) return 0.0f;
+    float h3 = h * h * h;
+    float k = 8.0f / (kPi * h3);
+    float gf;
+    if (q <= 0.5f) {
+        gf = k * (18.0f * q * q - 12.0f * q);
+    } else {
+        float omq = 1.0f - q;
+        gf = k * -6.0f * omq * omq;
+    }
+    return gf / (h * r);
+}
+
+// p / (rho * rho) for pressure_force, or NaN when rho <= 1e-6 (the shader
+// skips such neighbours, pressure_force.comp:64).
+__device__ __forceinline__ float pressure_over_rho2(float p, float rho) {
+    return rho > kEpsR ? p / (rho * rho) : __int_as_float(0x7fffffff);
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// Fixed-order FP64 sum of one value per thread of a 256-thread block:
+// warp halving tree (lane l + lane l^m, m = 16..1), then the 8 warp sums in a
+// halving tree (m = 4, 2, 1).  Result valid in thread 0.  `smem` holds 8
+// doubles.  The host oracle (fo_det_sum) reproduces this order.
+__device__ __forceinline__ double block_tree256(double v, double* smem) {
+    for (int m = 16; m >= 1; m >>= 1) v = v + __shfl_xor_sync(kFull, v, m);
+    const int warp = threadIdx.x >> 5;
+    if (lane_id() == 0) smem[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0) {
+        double w = lane_id() < 8 ? smem[lane_id()] : 0.0;
+        for (int m = 4; m >= 1; m >>= 1) w = w + __shfl_xor_sync(kFull, w, m);
+        r = w;
+    }
+    __syncthreads();
+    return r;
+}
+
+// Final stage of the fixed-order sum over `chunks` partials: thread t adds
+// partials t, t+256, ... in order, then block_tree256.  Valid in thread 0.
+__device__ __forceinline__ double block_final_sum(const double* partials, uint32_t chunks,
+                                                  double* smem) {
+    double s = 0.0;
+    for (uint32_t c = threadIdx.x; c < chunks; c += 256) s = s + __ldcg(partials + c);
+    return block_tree256(s, smem);
+}
+
+// "Last block" ticket: returns true in every thread of the block that
+// finished last.  Each block must have written its partials before calling.
+__device__ __forceinline__ bool last_block_done(uint32_t* counter, uint32_t nblocks) {
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = atomicAdd(counter, 1u);
+        s_last = (t == nblocks - 1);
+    }
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
+}
+
+}  // namespace fe

@@ -1,0 +1,605 @@
+// fe_kernels.cu — the DFSPH passes as sm_100a kernels.
+//
+// One 256-thread block per chunk of <= 256 particles of one scene.  Each
+// kernel restates one reference shader (cited per kernel); arithmetic is in
+// the shader's order with no contraction (see fe_common.cuh), so results
+// equal the host oracle bit for bit.
+//
+// Neighbour access.  density_alpha walks the 27 hash buckets exactly like the
+// shaders (z, y, x offsets; bucket walk in sorted order; r^2 <= h^2) and, in
+// the same pass, records for every particle the neighbours with r > 1e-6 in
+// walk order together with the gradient scale grad_factor / (h r) of
+// kernel_grad.  Positions do not move until the next neighbour search, so the
+// ~18 later neighbour passes of the substep read this list (8 bytes per pair,
+// coalesced: entry k of particle i at k * n_total + i) instead of re-walking
+// ~216 candidates; they visit the same pairs in the same order and therefore
+// produce identical sums.  A particle with more than kNbrCap neighbours keeps
+// walking the buckets in every pass.
+#include "fe_common.cuh"
+#include "fe_kernels.h"
+
+namespace fe {
+
+__device__ __forceinline__ bool chunk_of(const Bufs& B, uint32_t& i, uint32_t& s,
+                                         uint32_t& chunk) {
+    chunk = blockIdx.x;
+    uint4 c = B.chunks[chunk];
+    s = c.z;
+    i = c.x + threadIdx.x;
+    return threadIdx.x < c.y;
+}
+
+// The bucket walk of the shaders (e.g. density_and_alpha.comp:31-63) over the
+// {start, end} table.  f(j, r_vec, r2) is called for each candidate with
+// r2 <= h*h, in walk order.
+template <class F>
+__device__ __forceinline__ void walk(const Bufs& B, const DevParams& P, f3 pi, F&& f) {
+    const float h = P.h;
+    const float h2 = h * h;
+    const int cx = cell_coord(pi.x, h), cy = cell_coord(pi.y, h), cz = cell_coord(pi.z, h);
+    for (int z = -1; z <= 1; ++z)
+        for (int y = -1; y <= 1; ++y)
+            for (int x = -1; x <= 1; ++x) {
+                uint32_t k = P.table_base +
+                             cell_hash((int)((uint32_t)cx + (uint32_t)x),
+                                       (int)((uint32_t)cy + (uint32_t)y),
+                                       (int)((uint32_t)cz + (uint32_t)z), P.T);
+                uint2 cell = B.cells[k];
+                if (cell.x == kEmpty) continue;
+                for (uint32_t j = cell.x; j < cell.y; ++j) {
+                    f3 rv = sub(pi, xyz(__ldg(B.pos_b + j)));
+                    float r2 = dot(rv, rv);
+                    if (r2 > h2) continue;
+                    f(j, rv, r2);
+                }
+            }
+}
+
+// Neighbours with r > 1e-6 in walk order: f(j, r_vec, grad_scale).
+template <class F>
+__device__ __forceinline__ void for_each_neighbor(const Bufs& B, const DevParams& P, uint32_t i,
+                                                  f3 pi, F&& f) {
+    const uint32_t cnt = B.nbr_count[i];
+    if (cnt <= kNbrCap) {
+        const uint2* e = B.nbr + i;
+        const uint32_t stride = B.n_total;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            uint2 v = __ldg(e + (size_t)k * stride);
+            f3 rv = sub(pi, xyz(__ldg(B.pos_b + v.x)));
+            f(v.x, rv, __uint_as_float(v.y));
+        }
+    } else {
+        const float h = P.h;
+        walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
+            float r = sqrtf(r2);
+            if (r > kEpsR) f(j, rv, kernel_grad_scale(r, h));
+        });
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Neighbour search: spatial_hash.comp, grid_offsets.comp, reorder.comp.
+// ---------------------------------------------------------------------------
+__global__ void k_fill_u32(uint32_t* p, uint32_t v, size_t count) {
+    size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) p[i] = v;
+}
+
+__global__ void k_fill_cells(uint2* p, size_t count) {
+    size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        p[i] = make_uint2(kEmpty, kEmpty);
+}
+
+// spatial_hash.comp:23-36 (the sentinel tail is written once at creation and
+// never changes).
+__global__ void __launch_bounds__(kBlock) k_hash(Bufs B) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    float4 p = __ldg(B.pos_a + i);
+    const float h = P.h;
+    B.keys[i] = P.table_base + cell_hash(cell_coord(p.x, h), cell_coord(p.y, h),
+                                         cell_coord(p.z, h), P.T);
+    B.vals[i] = i;
+}
+
+// grid_offsets.comp:20-33, also recording where each bucket ends so that the
+// walk needs no hash comparison.
+__global__ void k_offsets(Bufs B) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B.n_total) return;
+    uint32_t key = B.keys[i];
+    if (key >= B.T_total) return;
+    uint32_t prev = i == 0 ? kEmpty : B.keys[i - 1];
+    uint32_t next = i + 1 == B.n_total ? kEmpty : B.keys[i + 1];
+    if (key != prev) B.cells[key].x = i;
+    if (key != next) B.cells[key].y = i + 1;
+}
+
+// reorder.comp:37-46.  FIXED mode also gathers the pressures into prs_tmp.
+// The neighbour list of the old order is invalidated: until density_alpha
+// rebuilds it, the neighbour passes walk the new buckets.
+__global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B.n_total) return;
+    uint32_t src = B.vals[i];
+    if (src >= B.n_total) src = i;  // unreachable for a valid permutation
+    B.nbr_count[i] = kNbrCap + 1;
+    B.pos_b[i] = __ldg(B.pos_a + src);
+    B.vel_b[i] = __ldg(B.vel_a + src);
+    if (carry_pressure) B.prs_tmp[i] = B.prs[src];
+}
+
+// FIXED mode: the gathered pressures become current; pr = p / rho^2 keeps
+// matching the (not yet recomputed) densities.
+__global__ void __launch_bounds__(kBlock) k_take_pressure(Bufs B) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B.n_total) return;
+    float p = B.prs_tmp[i];
+    B.prs[i] = p;
+    B.pr[i] = pressure_over_rho2(p, B.rho[i]);
+}
+
+// pr = p / rho^2 for all particles (after a host upload of p or rho).
+__global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B.n_total) return;
+    B.pr[i] = pressure_over_rho2(B.prs[i], B.rho[i]);
+}
+
+// ---------------------------------------------------------------------------
+// density_and_alpha.comp:14-72 + neighbour list.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_density_alpha(Bufs B) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    const float m = P.mass, h = P.h;
+    const f3 pi = xyz(__ldg(B.pos_b + i));
+    float density = 0.0f, sum_grad_sq = 0.0f;
+    f3 grad_sum = {0.0f, 0.0f, 0.0f};
+    uint32_t cnt = 0;
+    uint2* out = B.nbr + i;
+    const uint32_t stride = B.n_total;
+    walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
+        float r = sqrtf(r2);
+        float w = kernel_w(r, h);
+        density += m * w;
+        if (r > kEpsR) {
+            float g = kernel_grad_scale(r, h);
+            f3 grad = scale(g, rv);
+            f3 mg = scale(m, grad);
+            grad_sum = add(grad_sum, mg);
+            sum_grad_sq += dot(mg, mg);
+            if (cnt < kNbrCap) out[(size_t)cnt * stride] = make_uint2(j, __float_as_uint(g));
+            ++cnt;
+        }
+    });
+    B.rho[i] = density;
+    float a = sum_grad_sq + dot(grad_sum, grad_sum);
+    B.alpha[i] = a > kEpsR ? a : 0.0f;
+    B.nbr_count[i] = cnt;
+    B.pr[i] = pressure_over_rho2(B.prs[i], density);
+    if (cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
+}
+
+// ---------------------------------------------------------------------------
+// viscosity.comp:17-66: velocity_b in, velocity_a out.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_viscosity(Bufs B) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    const float m = P.mass, h = P.h;
+    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 vi = xyz(__ldg(B.vel_b + i));
+    f3 sum = {0.0f, 0.0f, 0.0f};
+    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float) {
+        float r2 = dot(rv, rv);
+        float r = sqrtf(r2);
+        float w = kernel_w(r, h);
+        f3 vd = sub(xyz(__ldg(B.vel_b + j)), vi);
+        sum = add(sum, scale_r(scale(m / __ldg(B.rho + j), vd), w));
+    });
+    f3 vv = add(vi, scale(P.visc, sum));
+    f3 g = {P.gx, P.gy, P.gz};
+    f3 vf = add(vv, scale_r(g, P.dt));
+    B.vel_a[i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// density_source_term.comp:16-74 (velocities = velocity_a).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_density_source(Bufs B) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    const float m = P.mass, dt = P.dt;
+    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 vi = xyz(B.vel_a[i]);
+    float div = 0.0f;
+    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
+        f3 grad = scale(g, rv);
+        f3 vd = sub(vi, xyz(B.vel_a[j]));
+        div += m * dot(vd, grad);
+    });
+    float rho_i = B.rho[i];
+    float source = 0.0f;
+    if (dt > kEpsR) source = ((P.rho0 - rho_i) / dt) - div;
+    B.src[i] = source;
+    B.prs[i] = 0.0f;
+    B.pr[i] = pressure_over_rho2(0.0f, rho_i);
+}
+
+// ---------------------------------------------------------------------------
+// divergence_source_term.comp:14-61 (velocities = velocity_a in REFERENCE
+// mode, velocity_b in FIXED mode).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_divergence_source(Bufs B, int fixed) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    const float m = P.mass;
+    const float4* __restrict__ vel = fixed ? B.vel_b : B.vel_a;
+    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 vi = xyz(vel[i]);
+    float div = 0.0f;
+    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
+        f3 grad = scale(g, rv);
+        f3 vd = sub(vi, xyz(vel[j]));
+        div += m * dot(vd, grad);
+    });
+    B.src[i] = -div;
+}
+
+// ---------------------------------------------------------------------------
+// pressure_force.comp:15-78.  pr[j] = p_j / rho_j^2 (NaN when rho_j <= 1e-6)
+// is maintained by every pass that writes p or rho.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_pressure_force(Bufs B, int which) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    if (which >= 0 && B.S[s].solve[which].done) return;
+    const DevParams& P = B.P[s];
+    const float m = P.mass;
+    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const float rho_i = B.rho[i], p_i = B.prs[i];
+    float p_rho_i = 0.0f;
+    if (rho_i > kEpsR) p_rho_i = p_i / (rho_i * rho_i);
+    f3 acc = {0.0f, 0.0f, 0.0f};
+    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
+        float p_rho_j = B.pr[j];
+        if (p_rho_j == p_rho_j) {
+            f3 grad = scale(g, rv);
+            float term = p_rho_i + p_rho_j;
+            acc = add(acc, scale(m * term, grad));
+        }
+    });
+    B.acc[i] = make_float4(-acc.x, -acc.y, -acc.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// pressure_update.comp:18-84, plus the solver control of the tolerance loop.
+// which = 0 (density solve), 1 (divergence solve), -1 (a bare stage call:
+// no control).  The per-particle predicted error of the pressure *before*
+// this update, e_i = max(-(dt * (s_i - Ap_i)), 0) (density) or
+// max(-(s_i - Ap_i), 0) (divergence), is summed in the fixed FP64 order; the
+// last block turns the per-scene sums into the metric, advances the
+// iteration count and sets the loop condition.
+// ---------------------------------------------------------------------------
+__device__ void solve_finish(Bufs& B, int which, cudaGraphConditionalHandle handle,
+                             int use_handle, double* smem) {
+    // Runs in the last block only: per scene, final sum and control update.
+    uint32_t any_open = 0;
+    uint32_t c0 = 0;
+    for (uint32_t s = 0; s < B.n_scenes; ++s) {
+        const DevParams& P = B.P[s];
+        SolveCtl& ctl = B.S[s].solve[which];
+        uint32_t nchunks = (P.n + kBlock - 1) / kBlock;
+        bool active = !ctl.done;
+        double sum = 0.0;
+        if (active && P.solver == 1u)
+            sum = block_final_sum(B.partials + c0, nchunks, smem);
+        if (threadIdx.x == 0 && active) {
+            ctl.iter += 1;
+            if (P.solver == 1u) {
+                double avg = sum / (double)P.n;
+                if (which == 1) avg = avg * (double)P.dt;
+                double metric = avg / (double)P.rho0;
+                ctl.metric = metric;
+                float tol = which == 0 ? P.tol_d : P.tol_v;
+                if (ctl.iter >= P.min_it && metric <= (double)tol) {
+                    ctl.done = 1;
+                } else if (ctl.iter >= P.max_it) {
+                    ctl.done = 1;
+                    ctl.cap_hit = 1;
+                }
+            } else {
+                if (ctl.iter >= ctl.K) ctl.done = 1;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && !ctl.done) any_open = 1;
+        c0 += nchunks;
+    }
+    if (threadIdx.x == 0) {
+        B.G->cond[which] = any_open;
+        if (use_handle) cudaGraphSetConditional(handle, any_open);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
+                                                            cudaGraphConditionalHandle handle,
+                                                            int use_handle) {
+    __shared__ double smem[8];
+    uint32_t i, s, c;
+    bool valid = chunk_of(B, i, s, c);
+    const DevParams& P = B.P[s];
+    const bool control = which >= 0;
+    const bool skip = control && B.S[s].solve[which].done;
+    double e_sum_in = 0.0;
+    if (valid && !skip) {
+        const float m = P.mass, dt = P.dt, omega = P.omega;
+        const f3 pi = xyz(__ldg(B.pos_b + i));
+        const f3 ai = xyz(B.acc[i]);
+        float sum_ap = 0.0f;
+        for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
+            f3 grad = scale(g, rv);
+            f3 ad = sub(ai, xyz(B.acc[j]));
+            sum_ap += m * dot(ad, grad);
+        });
+        const float alpha_i = B.alpha[i], rho_i = B.rho[i], s_i = B.src[i], p_i = B.prs[i];
+        float ap_i = dt * sum_ap;
+        float error = s_i - ap_i;
+        float p_new = p_i;
+        if (alpha_i > kEpsR && rho_i > kEpsR) {
+            float a_ii = -(dt / (rho_i * rho_i)) * alpha_i;
+            if (fabsf(a_ii) > 1e-20f) {
+                float corr = (omega * error) / a_ii;
+                float np = p_i + corr;
+                p_new = np > 0.0f ? np : 0.0f;
+                B.prs[i] = p_new;
+            }
+        }
+        B.pr[i] = pressure_over_rho2(p_new, rho_i);
+        if (control && P.solver == 1u) {
+            float e = which == 1 ? -error : -(dt * error);
+            e_sum_in = e > 0.0f ? (double)e : 0.0;
+        }
+    }
+    if (!control) return;
+    // Per-chunk partial of the fixed-order sum (uniform branch per block).
+    if (!skip && P.solver == 1u) {
+        double part = block_tree256(e_sum_in, smem);
+        if (threadIdx.x == 0) B.partials[c] = part;
+    }
+    if (last_block_done(&B.G->tickets[kTicketSolve], gridDim.x)) {
+        solve_finish(B, which, handle, use_handle, smem);
+        if (threadIdx.x == 0) B.G->tickets[kTicketSolve] = 0;
+    }
+}
+
+// Starts a solve: resets the per-scene control and sets the loop condition.
+__global__ void k_solve_begin(Bufs B, int which, cudaGraphConditionalHandle handle,
+                              int use_handle) {
+    if (threadIdx.x != 0) return;
+    uint32_t any_open = 0;
+    uint32_t cap = 0;
+    for (uint32_t s = 0; s < B.n_scenes; ++s) {
+        const DevParams& P = B.P[s];
+        SolveCtl& ctl = B.S[s].solve[which];
+        uint32_t want = (P.solver == 1u) ? P.max_it
+                                         : (which == 0 ? B.S[s].iters_rho : B.S[s].iters_div);
+        cap = want > cap ? want : cap;
+        ctl.iter = 0;
+        ctl.cap_hit = 0;
+        ctl.metric = 0.0;
+        ctl.K = which == 0 ? B.S[s].iters_rho : B.S[s].iters_div;
+        ctl.done = (P.solver == 1u) ? (P.max_it == 0u) : (ctl.K == 0u);
+        if (!ctl.done) any_open = 1;
+    }
+    B.G->cond[which] = any_open;
+    B.G->body_runs[which] = 0;
+    B.G->body_cap[which] = cap + 2;
+    if (use_handle) cudaGraphSetConditional(handle, any_open);
+}
+
+// Last node of a WHILE body: counts executions and ends the loop after a
+// hard bound even if the solver control above misbehaved, so a frame graph
+// always terminates.  Raises FE_STATS_LOOKBACK_TIMEOUT when it has to act.
+__global__ void k_loop_guard(Bufs B, int which, cudaGraphConditionalHandle handle) {
+    if (threadIdx.x != 0) return;
+    uint32_t runs = ++B.G->body_runs[which];
+    if (runs >= B.G->body_cap[which]) {
+        cudaGraphSetConditional(handle, 0);
+        B.G->cond[which] = 0;
+        atomicOr(&B.G->flags, 0x4u);
+    }
+}
+
+// Ends a solve: records iterations used, residual and cap hits.
+__global__ void k_solve_end(Bufs B, int which) {
+    if (threadIdx.x != 0) return;
+    for (uint32_t s = 0; s < B.n_scenes; ++s) {
+        SceneState& S = B.S[s];
+        SolveCtl& ctl = S.solve[which];
+        S.last_iters[which] = ctl.iter;
+        S.last_metric[which] = ctl.metric;
+        S.total_iters[which] += ctl.iter;
+        if (ctl.cap_hit) {
+            S.cap_hits += 1;
+            atomicOr(&B.G->flags, 0x1u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pressure_integration.comp:16-77: position_b in, position_a and velocity_a
+// out.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_pressure_integration(Bufs B) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    const float dt = P.dt, r = P.radius;
+    const float rest = 0.5f, fric = 0.95f, eps = 0.001f;
+    f3 pos = xyz(__ldg(B.pos_b + i));
+    f3 vel = xyz(B.vel_a[i]);
+    f3 ap = xyz(B.acc[i]);
+    f3 nv = add(vel, scale_r(ap, dt));
+    f3 np = add(pos, scale_r(nv, dt));
+    if (np.y < P.bminy + r) {
+        np.y = P.bminy + r + eps; nv.y *= -rest; nv.x *= fric; nv.z *= fric;
+    } else if (np.y > P.bmaxy - r) {
+        np.y = P.bmaxy - r - eps; nv.y *= -rest; nv.x *= fric; nv.z *= fric;
+    }
+    if (np.x < P.bminx + r) {
+        np.x = P.bminx + r + eps; nv.x *= -rest; nv.y *= fric; nv.z *= fric;
+    } else if (np.x > P.bmaxx - r) {
+        np.x = P.bmaxx - r - eps; nv.x *= -rest; nv.y *= fric; nv.z *= fric;
+    }
+    if (np.z < P.bminz + r) {
+        np.z = P.bminz + r + eps; nv.z *= -rest; nv.x *= fric; nv.y *= fric;
+    } else if (np.z > P.bmaxz - r) {
+        np.z = P.bmaxz - r - eps; nv.z *= -rest; nv.x *= fric; nv.y *= fric;
+    }
+    B.pos_a[i] = make_float4(np.x, np.y, np.z, 1.0f);
+    B.vel_a[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+}
+
+// divergence_integration.comp:14-43 (velocity; colour is render-only).
+__global__ void __launch_bounds__(kBlock) k_divergence_integration(Bufs B, int fixed) {
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
+    const DevParams& P = B.P[s];
+    float4* vel = fixed ? B.vel_b : B.vel_a;
+    f3 nv = add(xyz(vel[i]), scale_r(xyz(B.acc[i]), P.dt));
+    vel[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// stats.comp:18-30 + FP64 means.  Per-chunk partials, combined per scene by
+// the last block (no fill pass needed, order fixed).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t fixed_point(float x, float scale) {
+    float v = x * scale;
+    if (!(v > 0.0f)) return 0u;
+    if (v >= 10000.0f) return 10000u;
+    return (uint32_t)v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upart) {
+    __shared__ double smem[8];
+    __shared__ uint32_t s_u[3][8];
+    uint32_t i, s, c;
+    bool valid = chunk_of(B, i, s, c);
+    const DevParams& P = B.P[s];
+    const float4* vel = fixed ? B.vel_b : B.vel_a;
+    uint32_t mx = 0, s1 = 0, s2 = 0, bad = 0;
+    double d1 = 0.0, d2 = 0.0;
+    if (valid) {
+        float4 v = vel[i];
+        float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+        mx = __float_as_uint(speed);
+        float rho = B.rho[i], src = B.src[i];
+        s1 = fixed_point(fabsf(rho - P.rho0), 1.0f);
+        s2 = fixed_point(fabsf(src), 10.0f);
+        d1 = fabs((double)rho - (double)P.rho0);
+        d2 = fabs((double)src);
+        bad = !(isfinite(speed) && isfinite(rho) && isfinite(src));
+    }
+    // integer parts: order-free
+    for (int m = 16; m >= 1; m >>= 1) {
+        mx = max(mx, __shfl_xor_sync(kFull, mx, m));
+        s1 += __shfl_xor_sync(kFull, s1, m);
+        s2 += __shfl_xor_sync(kFull, s2, m);
+        bad |= __shfl_xor_sync(kFull, bad, m);
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane_id() == 0) {
+        s_u[0][warp] = mx;
+        s_u[1][warp] = s1;
+        s_u[2][warp] = s2;
+    }
+    if (bad) atomicOr(&B.S[s].nonfinite, 1u);
+    double p1 = block_tree256(d1, smem);
+    double p2 = block_tree256(d2, smem);
+    if (threadIdx.x == 0) {
+        uint32_t a = 0, b = 0, d = 0;
+        for (int w = 0; w < 8; ++w) {
+            a = max(a, s_u[0][w]);
+            b += s_u[1][w];
+            d += s_u[2][w];
+        }
+        upart[c] = make_uint4(a, b, d, 0);
+        B.partials[2 * c] = p1;
+        B.partials[2 * c + 1] = p2;
+    }
+    if (last_block_done(&B.G->tickets[kTicketStats], gridDim.x)) {
+        uint32_t c0 = 0;
+        for (uint32_t sc = 0; sc < B.n_scenes; ++sc) {
+            const DevParams& Q = B.P[sc];
+            uint32_t nch = (Q.n + kBlock - 1) / kBlock;
+            // Two FP64 sums in the fixed order over this scene's chunks.
+            double t1 = 0.0, t2 = 0.0;
+            for (uint32_t k = threadIdx.x; k < nch; k += kBlock) {
+                t1 = t1 + __ldcg(B.partials + 2 * (c0 + k));
+                t2 = t2 + __ldcg(B.partials + 2 * (c0 + k) + 1);
+            }
+            double f1 = block_tree256(t1, smem);
+            double f2 = block_tree256(t2, smem);
+            if (threadIdx.x == 0) {
+                uint32_t a = 0, b = 0, d = 0;
+                for (uint32_t k = 0; k < nch; ++k) {
+                    uint4 u = __ldcg(upart + c0 + k);
+                    a = max(a, u.x);
+                    b += u.y;
+                    d += u.z;
+                }
+                SceneState& S = B.S[sc];
+                S.stats[0] = a;
+                S.stats[1] = b;
+                S.stats[2] = d;
+                S.stats_f64[0] = f1 / (double)Q.n;
+                S.stats_f64[1] = f2 / (double)Q.n;
+            }
+            c0 += nch;
+        }
+        if (threadIdx.x == 0) B.G->tickets[kTicketStats] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Frame prologue (renderer/mod.rs:231-267): adaptive CFL dt and early-exit
+// iteration choice from the previous frame's stats.  One thread per scene.
+// ---------------------------------------------------------------------------
+__global__ void k_frame_prologue(Bufs B) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= B.n_scenes) return;
+    DevParams& P = B.P[s];
+    SceneState& S = B.S[s];
+    float n = (float)P.n;
+    float max_speed = __uint_as_float(S.stats[0]);
+    float avg_de = (float)S.stats[1] / (1.0f * n);
+    float avg_ve = (float)S.stats[2] / (10.0f * n);
+    if (P.use_cfl && max_speed > 0.01f) {
+        float cfl = (P.cfl_lambda * P.h) / max_speed;
+        if (cfl < P.cfl_min) cfl = P.cfl_min;
+        if (cfl > P.cfl_max) cfl = P.cfl_max;
+        P.dt = fminf(cfl, P.dt * P.cfl_growth);
+    }
+    float rho0 = P.rho0;
+    float thr_d = P.eta_d_pct / 100.0f * rho0;
+    float thr_v = P.eta_v_pct / 100.0f * rho0;
+    bool early = P.use_thr && P.solver == 0u;
+    S.iters_rho = (early && avg_de < thr_d) ? 2u : P.k_rho;
+    S.iters_div = (early && avg_ve < thr_v) ? 1u : P.k_div;
+}
+
+__global__ void k_count_substep(Bufs B) {
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < B.n_scenes) B.S[s].substeps += 1;
+}
+
+}  // namespace fe

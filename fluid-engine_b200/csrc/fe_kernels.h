@@ -1,0 +1,36 @@
+// fe_kernels.h — declarations of the DFSPH kernels (fe_kernels.cu) and the
+// sort (fe_sort.cu) for the host driver.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fe_device.h"
+
+namespace fe {
+
+__global__ void k_fill_u32(uint32_t* p, uint32_t v, size_t count);
+__global__ void k_fill_cells(uint2* p, size_t count);
+__global__ void k_hash(Bufs B);
+__global__ void k_offsets(Bufs B);
+__global__ void k_reorder(Bufs B, int carry_pressure);
+__global__ void k_take_pressure(Bufs B);
+__global__ void k_refresh_pr(Bufs B);
+__global__ void k_density_alpha(Bufs B);
+__global__ void k_viscosity(Bufs B);
+__global__ void k_density_source(Bufs B);
+__global__ void k_divergence_source(Bufs B, int fixed);
+__global__ void k_pressure_force(Bufs B, int which);
+__global__ void k_pressure_update(Bufs B, int which, cudaGraphConditionalHandle handle,
+                                  int use_handle);
+__global__ void k_solve_begin(Bufs B, int which, cudaGraphConditionalHandle handle,
+                              int use_handle);
+__global__ void k_solve_end(Bufs B, int which);
+__global__ void k_loop_guard(Bufs B, int which, cudaGraphConditionalHandle handle);
+__global__ void k_pressure_integration(Bufs B);
+__global__ void k_divergence_integration(Bufs B, int fixed);
+__global__ void k_stats(Bufs B, int fixed, uint4* upart);
+__global__ void k_frame_prologue(Bufs B);
+__global__ void k_count_substep(Bufs B);
+
+}  // namespace fe

@@ -74,6 +74,7 @@ FE_STEP_NO_GRAPH = 0x2
 FE_STATS_ITERATION_CAP_HIT = 0x1
 FE_STATS_NEIGHBOR_OVERFLOW = 0x2
 FE_STATS_LOOKBACK_TIMEOUT = 0x4
+FE_STATS_NON_FINITE = 0x8
 
 FE_MAX_PARTICLES = 1 << 26
 

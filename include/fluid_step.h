@@ -32,6 +32,12 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#define FE_API __attribute__((visibility("default")))
+#else
+#define FE_API
+#endif
+
 #define FE_ABI_VERSION 1u
 
 /* ------------------------------------------------------------------------- */
@@ -163,6 +169,7 @@ typedef struct fe_stats {
 #define FE_STATS_ITERATION_CAP_HIT   0x1u /* a tolerance solve hit the cap   */
 #define FE_STATS_NEIGHBOR_OVERFLOW   0x2u /* some particle exceeded the list */
 #define FE_STATS_LOOKBACK_TIMEOUT    0x4u /* a bounded device wait gave up   */
+#define FE_STATS_NON_FINITE          0x8u /* NaN/Inf seen by the stats pass  */
 
 /* Fields addressable by fe_upload / fe_download.  Names follow
  * `GpuPhysicsData` (particle.rs:137-161).  Vector fields travel as 4 floats
@@ -195,21 +202,21 @@ typedef struct fe_ctx fe_ctx;
 /* Library                                                                   */
 /* ------------------------------------------------------------------------- */
 /* ABI version of the loaded library (FE_ABI_VERSION). */
-uint32_t fe_abi_version(void);
+FE_API uint32_t fe_abi_version(void);
 
 /* Text of a status code.  Static storage. */
-const char* fe_status_string(fe_status status);
+FE_API const char* fe_status_string(fe_status status);
 
 /* Last error message recorded on this host thread (empty if none). */
-const char* fe_last_error(void);
+FE_API const char* fe_last_error(void);
 
 /* Defaults of `Scene::new()` (src/core/scene.rs:14-86) and `AppUI::new()`
  * (src/renderer/ui.rs:31-49), plus the extension defaults. */
-void fe_default_params(fe_params* out);
+FE_API void fe_default_params(fe_params* out);
 
 /* Validates a parameter block (finite values, h > 0, mass > 0, box_min <
  * box_max, iteration bounds, enums).  The reference has no validation. */
-fe_status fe_validate_params(const fe_params* params);
+FE_API fe_status fe_validate_params(const fe_params* params);
 
 /* ------------------------------------------------------------------------- */
 /* Context = GpuPhysicsData + ComputePipelines                               */
@@ -220,36 +227,36 @@ fe_status fe_validate_params(const fe_params* params);
  * particle.rs:193-204), hash table of T = next_pow2(n) (particle.rs:255).
  * n must be in 1..FE_MAX_PARTICLES. */
 #define FE_MAX_PARTICLES (1u << 26)
-fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
+FE_API fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
                     const float* vel_xyz, int device, fe_ctx** out);
 
 /* Frees everything owned by ctx.  NULL is accepted. */
-fe_status fe_destroy(fe_ctx* ctx);
+FE_API fe_status fe_destroy(fe_ctx* ctx);
 
 /* `Resources::sync_with_scene` (src/renderer/resources.rs:85-92): replaces
  * the parameter block used by later calls. */
-fe_status fe_set_params(fe_ctx* ctx, const fe_params* params);
-fe_status fe_get_params(const fe_ctx* ctx, fe_params* out);
+FE_API fe_status fe_set_params(fe_ctx* ctx, const fe_params* params);
+FE_API fe_status fe_get_params(const fe_ctx* ctx, fe_params* out);
 
 /* `ComputeStep::prepare` for all passes (renderer/mod.rs:137-192): binds
  * buffers and sizes launches.  Must precede the stage calls and fe_step. */
-fe_status fe_prepare(fe_ctx* ctx);
+FE_API fe_status fe_prepare(fe_ctx* ctx);
 
 /* Particle count N and table size T of the context. */
-fe_status fe_get_size(const fe_ctx* ctx, uint32_t* n, uint32_t* table_size);
+FE_API fe_status fe_get_size(const fe_ctx* ctx, uint32_t* n, uint32_t* table_size);
 
 /* CUDA stream of the context (cudaStream_t as void*). */
-void* fe_get_stream(fe_ctx* ctx);
+FE_API void* fe_get_stream(fe_ctx* ctx);
 
 /* Waits for all work enqueued on the context (the reference's fence wait,
  * convergence_benchmark.rs:156-162). */
-fe_status fe_synchronize(fe_ctx* ctx);
+FE_API fe_status fe_synchronize(fe_ctx* ctx);
 
 /* Copies a field between host memory and the context (bytes = element count
  * of the field × element size, see fe_field).  Enqueued on the context's
  * stream; download completes before returning. */
-fe_status fe_upload(fe_ctx* ctx, fe_field field, const void* src, size_t bytes);
-fe_status fe_download(fe_ctx* ctx, fe_field field, void* dst, size_t bytes);
+FE_API fe_status fe_upload(fe_ctx* ctx, fe_field field, const void* src, size_t bytes);
+FE_API fe_status fe_download(fe_ctx* ctx, fe_field field, void* dst, size_t bytes);
 
 /* ------------------------------------------------------------------------- */
 /* Stage entry points: one per `ComputeStep::execute`                         */
@@ -257,29 +264,29 @@ fe_status fe_download(fe_ctx* ctx, fe_field field, void* dst, size_t bytes);
 /* NeighborSearch::execute (neighbor_search.rs:176-231): spatial_hash.comp,
  * sort (radix or bitonic per params.sort_algorithm), fill(grid_start,
  * 0xFFFFFFFF), grid_offsets.comp, reorder.comp. */
-fe_status fe_neighbor_search(fe_ctx* ctx);
+FE_API fe_status fe_neighbor_search(fe_ctx* ctx);
 /* DensityAlphaPipeline::execute (density_alpha.rs:56-63; density_and_alpha.comp) */
-fe_status fe_density_alpha(fe_ctx* ctx);
+FE_API fe_status fe_density_alpha(fe_ctx* ctx);
 /* ViscosityPipeline::execute (viscosity.rs:56-64; viscosity.comp) */
-fe_status fe_viscosity(fe_ctx* ctx);
+FE_API fe_status fe_viscosity(fe_ctx* ctx);
 /* DensitySourceTermPipeline::execute (density_source_term.rs:53-62) */
-fe_status fe_density_source(fe_ctx* ctx);
+FE_API fe_status fe_density_source(fe_ctx* ctx);
 /* PressureForcePipeline::execute (pressure_force_pipeline.rs:56-64) */
-fe_status fe_pressure_force(fe_ctx* ctx);
+FE_API fe_status fe_pressure_force(fe_ctx* ctx);
 /* PressureUpdatePipeline::execute (pressure_update_pipeline.rs:60-69) */
-fe_status fe_pressure_update(fe_ctx* ctx);
+FE_API fe_status fe_pressure_update(fe_ctx* ctx);
 /* PressureIntegrationPipeline::execute (pressure_integration_pipeline.rs:56-65) */
-fe_status fe_pressure_integration(fe_ctx* ctx);
+FE_API fe_status fe_pressure_integration(fe_ctx* ctx);
 /* DivergenceSourceTermPipeline::execute (divergence_source_term.rs:51-60) */
-fe_status fe_divergence_source(fe_ctx* ctx);
+FE_API fe_status fe_divergence_source(fe_ctx* ctx);
 /* DivergenceIntegrationPipeline::execute (divergence_integration.rs:56-64) */
-fe_status fe_divergence_integration(fe_ctx* ctx);
+FE_API fe_status fe_divergence_integration(fe_ctx* ctx);
 /* StatsPipeline::execute (stats_pipeline.rs:54-66): fill(0) + stats.comp. */
-fe_status fe_stats_pass(fe_ctx* ctx);
+FE_API fe_status fe_stats_pass(fe_ctx* ctx);
 
 /* Reads the stats of the last stats pass (host read of `stats_buffer`,
  * renderer/mod.rs:231-236).  Synchronises the context's stream. */
-fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
+FE_API fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
 
 /* ------------------------------------------------------------------------- */
 /* Whole step                                                                */
@@ -298,7 +305,7 @@ fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
  * The frame is replayed from a CUDA graph (conditional WHILE nodes for the
  * tolerance solver) unless FE_STEP_NO_GRAPH.  `out` may be NULL; when given,
  * the call synchronises and fills it. */
-fe_status fe_step(fe_ctx* ctx, uint32_t n_substeps, uint32_t flags, fe_stats* out);
+FE_API fe_status fe_step(fe_ctx* ctx, uint32_t n_substeps, uint32_t flags, fe_stats* out);
 
 /* ------------------------------------------------------------------------- */
 /* Sorting                                                                   */
@@ -314,12 +321,12 @@ fe_status fe_step(fe_ctx* ctx, uint32_t n_substeps, uint32_t flags, fe_stats* ou
  *     n must be a power of two; not stable (same network, same result as
  *     the reference for the same input).
  * Scratch is allocated on first use per (device, size class) and kept. */
-fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
+FE_API fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
                         uint32_t key_bits, int algorithm, void* stream);
 
 /* Same as fe_sort_pairs with host arrays: copies in, sorts, copies out
  * (in place). */
-fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* values, uint32_t n,
+FE_API fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* values, uint32_t n,
                              uint32_t key_bits, int algorithm);
 
 #ifdef __cplusplus
