@@ -172,8 +172,11 @@ def run_gpu(args) -> None:
     h = sim.data.handle
     stream = torch.cuda.ExternalStream(lib.fe_get_stream(h), device=local)
 
+    # --eager launches each frame's kernels directly (FE_STEP_NO_GRAPH); the
+    # kernels and their work are the same as in the graph replay.
+    step_flags = _abi.FE_STEP_NO_GRAPH if args.eager else 0
     for _ in range(args.warmup):
-        st = sim.step(1)
+        st = sim.step(1, step_flags)
     barrier(world)
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -182,7 +185,7 @@ def run_gpu(args) -> None:
     with ClockSampler(local) as clocks:
         start.record(stream)
         for _ in range(args.steps):
-            rc = lib.fe_step(h, 1, 0, None)
+            rc = lib.fe_step(h, 1, step_flags, None)
             if rc:
                 raise RuntimeError(f"fe_step failed: {rc}")
         end.record(stream)
@@ -209,7 +212,7 @@ def run_gpu(args) -> None:
     t0 = time.perf_counter()
     for _ in range(args.steps):
         lib.fe_set_params(h, ctypes.byref(p))
-        lib.fe_step(h, 1, 0, None)
+        lib.fe_step(h, 1, step_flags, None)
         lib.fe_read_stats(h, ctypes.byref(stats_host))
         lib.fe_download(h, _abi.FE_FIELD_POSITION_A, pos_host.ctypes.data_as(ctypes.c_void_p),
                         pos_host.nbytes)
@@ -308,7 +311,8 @@ def run_gpu(args) -> None:
                        "mode": "FIXED", "solver": "tolerance 0.1%/0.1%, FP64 residuals",
                        "avg_jacobi_iterations": {"density": iters_d, "divergence": iters_v},
                        "l2": "working set > L2 (no flush needed)",
-                       "timing": "CUDA events on the context stream, graph replay per frame"},
+                       "timing": "CUDA events on the context stream, "
+                                 + ("eager launches" if args.eager else "graph replay per frame")},
             "e2e": {"value": e2e, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": ctypes.sizeof(_abi.FeParams),
                     "d2h_bytes_per_step": n * 16 + 192,
@@ -397,6 +401,8 @@ def main():
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--reference-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch frames without CUDA graphs (for profilers)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -549,13 +549,31 @@ __global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upar
             }
             double f1 = block_tree256(t1, smem);
             double f2 = block_tree256(t2, smem);
+            // integer partials: max and wrapping sums, order-free
+            uint32_t a = 0, b = 0, d = 0;
+            for (uint32_t k = threadIdx.x; k < nch; k += kBlock) {
+                uint4 u = __ldcg(upart + c0 + k);
+                a = max(a, u.x);
+                b += u.y;
+                d += u.z;
+            }
+            for (int m = 16; m >= 1; m >>= 1) {
+                a = max(a, __shfl_xor_sync(kFull, a, m));
+                b += __shfl_xor_sync(kFull, b, m);
+                d += __shfl_xor_sync(kFull, d, m);
+            }
+            if (lane_id() == 0) {
+                s_u[0][threadIdx.x >> 5] = a;
+                s_u[1][threadIdx.x >> 5] = b;
+                s_u[2][threadIdx.x >> 5] = d;
+            }
+            __syncthreads();
             if (threadIdx.x == 0) {
-                uint32_t a = 0, b = 0, d = 0;
-                for (uint32_t k = 0; k < nch; ++k) {
-                    uint4 u = __ldcg(upart + c0 + k);
-                    a = max(a, u.x);
-                    b += u.y;
-                    d += u.z;
+                a = b = d = 0;
+                for (int w = 0; w < 8; ++w) {
+                    a = max(a, s_u[0][w]);
+                    b += s_u[1][w];
+                    d += s_u[2][w];
                 }
                 SceneState& S = B.S[sc];
                 S.stats[0] = a;
