@@ -24,6 +24,7 @@
 
 #include "../../include/fluid_step.h"
 #include "fe_device.h"
+#include "fe_error.h"
 #include "fe_kernels.h"
 #include "fe_sort.h"
 
@@ -33,13 +34,17 @@ namespace {
 
 thread_local std::string g_last_error;
 
-void set_error(const char* fmt, ...) {
+void set_error_v(const char* fmt, va_list ap) {
     char buf[512];
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    g_last_error = buf;
+}
+
+void set_error(const char* fmt, ...) {
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
+    set_error_v(fmt, ap);
     va_end(ap);
-    g_last_error = buf;
 }
 
 #define FE_CUDA(call)                                                                   \
@@ -561,6 +566,13 @@ fe_status collect_stats(fe_ctx* c, fe_stats* out) {
 }
 
 }  // namespace
+
+void fe_set_error_message(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    set_error_v(fmt, ap);
+    va_end(ap);
+}
 
 // ---------------------------------------------------------------------------
 // C ABI

@@ -257,7 +257,10 @@ SIGNATURES = {
     "fe_step": (c_int, [CTX, c_uint32, c_uint32, POINTER(FeStats)]),
     "fe_sort_pairs": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p]),
     "fe_sort_pairs_host": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int]),
+    "fe_sort_pairs_noalloc": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p]),
 }
+
+FE_SORT_NOALLOC_MAX_PAIRS = 1 << 20
 
 
 def _declare(lib) -> None:

@@ -329,6 +329,23 @@ FE_API fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
 FE_API fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* values, uint32_t n,
                              uint32_t key_bits, int algorithm);
 
+/* Radix sort that allocates nothing.  No counterpart in the reference: it is
+ * for callers that cannot let a library allocate device memory — a frame
+ * loop that must not stall (cudaMalloc/cudaFree synchronise the device),
+ * work recorded by stream capture in global mode (allocation is refused while
+ * such a capture is open), or a host that budgets all device memory itself.
+ * Same result as fe_sort_pairs with FE_SORT_RADIX.  Its scratch is a static
+ * device array of about 9 MiB that every GPU loading the library holds until
+ * the process exits; n above FE_SORT_NOALLOC_MAX_PAIRS returns
+ * FE_ERR_CAPACITY.  The first call on a device looks up the array's device
+ * address (make that first call before any stream capture).  All calls share
+ * the array, so calls that overlap on the GPU (concurrent streams, devices
+ * excepted) race; serialise them on one stream.  keys and values are device
+ * pointers of the current device; work is enqueued on `stream`. */
+#define FE_SORT_NOALLOC_MAX_PAIRS (1u << 20)
+FE_API fe_status fe_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
+                                       uint32_t key_bits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
