@@ -358,6 +358,27 @@ def cpu_baseline(workload: str, w=None, frames: int = 1):
             "sample": f"{frames} frame(s) of {workload} ({pos.shape[0]} particles) from rest"}
 
 
+def run_profile_passes(args) -> None:
+    """A short, profiler-friendly run: a few frames launched eagerly
+    (FE_STEP_NO_GRAPH), then one launch of each hot pass on the same state."""
+    from fluid_step import _abi, scene
+    from fluid_step.pipelines import Simulation
+    w = scene.workload(args.workload)
+    sim = Simulation(w.positions(), w.params)
+    for _ in range(3):
+        st = sim.step(1, _abi.FE_STEP_NO_GRAPH)
+    lib, h = sim.data._lib, sim.data.handle
+    for name in ("fe_pressure_force", "fe_pressure_update", "fe_neighbor_search",
+                 "fe_density_alpha", "fe_viscosity", "fe_density_source"):
+        rc = getattr(lib, name)(h)
+        if rc:
+            raise RuntimeError(f"{name}: {rc}")
+    lib.fe_synchronize(h)
+    print(json.dumps({"profile_passes": args.workload,
+                      "iterations": [st.density_iterations, st.divergence_iterations]}))
+    sim.close()
+
+
 def run_reference(args) -> None:
     rank, world, _ = dist_env()
     if rank != 0:
@@ -401,12 +422,16 @@ def main():
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--reference-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-passes", action="store_true",
+                    help="eager frames, then one launch of each hot pass (for ncu -k)")
     ap.add_argument("--eager", action="store_true",
                     help="launch frames without CUDA graphs (for profilers)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile_passes:
+        run_profile_passes(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -704,7 +704,7 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
         (s = dev_alloc(c, &B.acc, n)) || (s = dev_alloc(c, &B.rho, n)) ||
         (s = dev_alloc(c, &B.alpha, n)) || (s = dev_alloc(c, &B.src, n)) ||
         (s = dev_alloc(c, &B.prs, n)) || (s = dev_alloc(c, &B.prs_tmp, n)) ||
-        (s = dev_alloc(c, &B.pr, n)) || (s = dev_alloc(c, &B.keys, c->T)) ||
+        (s = dev_alloc(c, &B.keys, c->T)) ||
         (s = dev_alloc(c, &B.vals, c->T)) || (s = dev_alloc(c, &B.cells, c->T)) ||
         (s = dev_alloc(c, &B.nbr_count, n)) || (s = dev_alloc(c, &B.nbr, (size_t)kNbrCap * n)) ||
         (s = dev_alloc(c, &chunks_d, nchunks)) || (s = dev_alloc(c, &B.P, 1)) ||
@@ -844,7 +844,9 @@ fe_status fe_upload(fe_ctx* c, fe_field f, const void* src, size_t bytes) {
     }
     FE_CUDA(cudaSetDevice(c->device));
     FE_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c->stream));
-    if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY) return run_refresh_pr(c);
+    // pos_b.w caches p / rho^2 for pressure_force.
+    if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY || f == FE_FIELD_POSITION_B)
+        return run_refresh_pr(c);
     return FE_OK;
 }
 
@@ -867,6 +869,13 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
         FE_CUDA(cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, c->stream));
     }
     FE_CUDA(cudaStreamSynchronize(c->stream));
+    if (f == FE_FIELD_POSITION_B) {
+        // The device keeps p / rho^2 in w; the reference's position_b.w is the
+        // copied position_a.w, which is always 1 (particle.rs:171,
+        // pressure_integration.comp:75).
+        float* v = static_cast<float*>(dst);
+        for (uint32_t i = 0; i < c->n; ++i) v[4 * i + 3] = 1.0f;
+    }
     return FE_OK;
 }
 

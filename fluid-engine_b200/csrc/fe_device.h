@@ -72,8 +72,8 @@ enum Ticket : int { kTicketStats = 0, kTicketSolve = 1, kTicketHist = 2 };
 
 // Kernel-side view of every buffer of a context (passed by value).
 struct Bufs {
-    float4 *pos_a, *pos_b, *vel_a, *vel_b, *acc;
-    float *rho, *alpha, *src, *prs, *prs_tmp, *pr;
+    float4 *pos_a, *pos_b, *vel_a, *vel_b, *acc;  // pos_b.w = p / rho^2 (NaN: rho <= 1e-6)
+    float *rho, *alpha, *src, *prs, *prs_tmp;
     uint32_t *keys, *vals;      // grid_entries (hash, index), T_total
     uint2* cells;               // {start, end} per table slot, T_total
     uint32_t* nbr_count;        // per particle; > kNbrCap = walk instead

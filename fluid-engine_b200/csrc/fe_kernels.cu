@@ -55,27 +55,67 @@ __device__ __forceinline__ void walk(const Bufs& B, const DevParams& P, f3 pi, F
             }
 }
 
-// Neighbours with r > 1e-6 in walk order: f(j, r_vec, grad_scale).
-template <class F>
+// Streaming read of a neighbour-list entry: read once per pass, so it
+// bypasses L1 and carries an evict-first L2 policy, leaving the caches to the
+// gathered neighbour data.
+__device__ __forceinline__ uint64_t evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ uint2 ld_list(const uint2* p, uint64_t pol) {
+    uint2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                 : "=r"(v.x), "=r"(v.y)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+
+// Neighbours with r > 1e-6 in walk order: f(j, r_vec, grad_scale, pos_j, d_j)
+// where pos_j = pos_b[j] (w = p_j / rho_j^2) and d_j = gather(j).  List
+// entries are consumed four at a time with all their loads issued before the
+// arithmetic, which then runs strictly in list order.
+template <class G, class F>
 __device__ __forceinline__ void for_each_neighbor(const Bufs& B, const DevParams& P, uint32_t i,
-                                                  f3 pi, F&& f) {
+                                                  f3 pi, G&& gather, F&& f) {
     const uint32_t cnt = B.nbr_count[i];
     if (cnt <= kNbrCap) {
         const uint2* e = B.nbr + i;
-        const uint32_t stride = B.n_total;
-        for (uint32_t k = 0; k < cnt; ++k) {
-            uint2 v = __ldg(e + (size_t)k * stride);
-            f3 rv = sub(pi, xyz(__ldg(B.pos_b + v.x)));
-            f(v.x, rv, __uint_as_float(v.y));
+        const size_t stride = B.n_total;
+        const uint64_t pol = evict_first_policy();
+        uint32_t k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            uint2 v0 = ld_list(e + (k + 0) * stride, pol);
+            uint2 v1 = ld_list(e + (k + 1) * stride, pol);
+            uint2 v2 = ld_list(e + (k + 2) * stride, pol);
+            uint2 v3 = ld_list(e + (k + 3) * stride, pol);
+            float4 q0 = __ldg(B.pos_b + v0.x), q1 = __ldg(B.pos_b + v1.x);
+            float4 q2 = __ldg(B.pos_b + v2.x), q3 = __ldg(B.pos_b + v3.x);
+            auto d0 = gather(v0.x);
+            auto d1 = gather(v1.x);
+            auto d2 = gather(v2.x);
+            auto d3 = gather(v3.x);
+            f(v0.x, sub(pi, xyz(q0)), __uint_as_float(v0.y), q0, d0);
+            f(v1.x, sub(pi, xyz(q1)), __uint_as_float(v1.y), q1, d1);
+            f(v2.x, sub(pi, xyz(q2)), __uint_as_float(v2.y), q2, d2);
+            f(v3.x, sub(pi, xyz(q3)), __uint_as_float(v3.y), q3, d3);
+        }
+        for (; k < cnt; ++k) {
+            uint2 v = ld_list(e + k * stride, pol);
+            float4 q = __ldg(B.pos_b + v.x);
+            f(v.x, sub(pi, xyz(q)), __uint_as_float(v.y), q, gather(v.x));
         }
     } else {
         const float h = P.h;
         walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
             float r = sqrtf(r2);
-            if (r > kEpsR) f(j, rv, kernel_grad_scale(r, h));
+            if (r > kEpsR) f(j, rv, kernel_grad_scale(r, h), __ldg(B.pos_b + j), gather(j));
         });
     }
 }
+
+struct NoData {};
 
 // ---------------------------------------------------------------------------
 // Neighbour search: spatial_hash.comp, grid_offsets.comp, reorder.comp.
@@ -126,7 +166,11 @@ __global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) 
     uint32_t src = B.vals[i];
     if (src >= B.n_total) src = i;  // unreachable for a valid permutation
     B.nbr_count[i] = kNbrCap + 1;
-    B.pos_b[i] = __ldg(B.pos_a + src);
+    // pos_b.w holds p / rho^2 of slot i (pressures and densities are not
+    // permuted here), so it is carried over.
+    float4 p = __ldg(B.pos_a + src);
+    p.w = B.pos_b[i].w;
+    B.pos_b[i] = p;
     B.vel_b[i] = __ldg(B.vel_a + src);
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
 }
@@ -138,50 +182,84 @@ __global__ void __launch_bounds__(kBlock) k_take_pressure(Bufs B) {
     if (i >= B.n_total) return;
     float p = B.prs_tmp[i];
     B.prs[i] = p;
-    B.pr[i] = pressure_over_rho2(p, B.rho[i]);
+    B.pos_b[i].w = pressure_over_rho2(p, B.rho[i]);
 }
 
 // pr = p / rho^2 for all particles (after a host upload of p or rho).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
-    B.pr[i] = pressure_over_rho2(B.prs[i], B.rho[i]);
+    B.pos_b[i].w = pressure_over_rho2(B.prs[i], B.rho[i]);
 }
 
 // ---------------------------------------------------------------------------
 // density_and_alpha.comp:14-72 + neighbour list.
+//
+// Two phases with the shader's summation order.  Phase 1 walks the 27
+// buckets and only records the in-range candidates (r^2 <= h^2) in shared
+// memory: a short loop that the lanes of a warp execute together.  Phase 2
+// visits the recorded candidates in order and does the expensive part
+// (sqrt, kernel, gradient, list entry) with the lanes in lockstep.  A
+// particle with more than kStage in-range candidates redoes everything in a
+// single-phase walk.
 // ---------------------------------------------------------------------------
+constexpr int kStage = 44;
+
+struct DensityAcc {
+    float density = 0.0f, sum_grad_sq = 0.0f;
+    f3 grad_sum = {0.0f, 0.0f, 0.0f};
+    uint32_t cnt = 0;
+};
+
+__device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, uint32_t j, f3 rv,
+                                             float r2, uint2* out, uint32_t stride) {
+    float r = sqrtf(r2);
+    float w = kernel_w(r, h);
+    a.density += m * w;
+    if (r > kEpsR) {
+        float g = kernel_grad_scale(r, h);
+        f3 grad = scale(g, rv);
+        f3 mg = scale(m, grad);
+        a.grad_sum = add(a.grad_sum, mg);
+        a.sum_grad_sq += dot(mg, mg);
+        if (a.cnt < kNbrCap) out[(size_t)a.cnt * stride] = make_uint2(j, __float_as_uint(g));
+        ++a.cnt;
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_density_alpha(Bufs B) {
+    __shared__ uint32_t s_cand[kStage][kBlock];
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
     const f3 pi = xyz(__ldg(B.pos_b + i));
-    float density = 0.0f, sum_grad_sq = 0.0f;
-    f3 grad_sum = {0.0f, 0.0f, 0.0f};
-    uint32_t cnt = 0;
     uint2* out = B.nbr + i;
     const uint32_t stride = B.n_total;
-    walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
-        float r = sqrtf(r2);
-        float w = kernel_w(r, h);
-        density += m * w;
-        if (r > kEpsR) {
-            float g = kernel_grad_scale(r, h);
-            f3 grad = scale(g, rv);
-            f3 mg = scale(m, grad);
-            grad_sum = add(grad_sum, mg);
-            sum_grad_sq += dot(mg, mg);
-            if (cnt < kNbrCap) out[(size_t)cnt * stride] = make_uint2(j, __float_as_uint(g));
-            ++cnt;
-        }
+    const int t = threadIdx.x;
+    // Phase 1: in-range candidates in walk order.
+    uint32_t n1 = 0;
+    walk(B, P, pi, [&](uint32_t j, f3, float) {
+        if (n1 < (uint32_t)kStage) s_cand[n1][t] = j;
+        ++n1;
     });
-    B.rho[i] = density;
-    float a = sum_grad_sq + dot(grad_sum, grad_sum);
-    B.alpha[i] = a > kEpsR ? a : 0.0f;
-    B.nbr_count[i] = cnt;
-    B.pr[i] = pressure_over_rho2(B.prs[i], density);
-    if (cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
+    DensityAcc a;
+    if (n1 <= (uint32_t)kStage) {
+        // Phase 2: the recorded candidates, same order.
+        for (uint32_t k = 0; k < n1; ++k) {
+            uint32_t j = s_cand[k][t];
+            f3 rv = sub(pi, xyz(__ldg(B.pos_b + j)));
+            density_term(a, m, h, j, rv, dot(rv, rv), out, stride);
+        }
+    } else {
+        walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) { density_term(a, m, h, j, rv, r2, out, stride); });
+    }
+    B.rho[i] = a.density;
+    float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
+    B.alpha[i] = al > kEpsR ? al : 0.0f;
+    B.nbr_count[i] = a.cnt;
+    B.pos_b[i].w = pressure_over_rho2(B.prs[i], a.density);
+    if (a.cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
 }
 
 // ---------------------------------------------------------------------------
@@ -195,13 +273,19 @@ __global__ void __launch_bounds__(kBlock) k_viscosity(Bufs B) {
     const f3 pi = xyz(__ldg(B.pos_b + i));
     const f3 vi = xyz(__ldg(B.vel_b + i));
     f3 sum = {0.0f, 0.0f, 0.0f};
-    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float) {
-        float r2 = dot(rv, rv);
-        float r = sqrtf(r2);
-        float w = kernel_w(r, h);
-        f3 vd = sub(xyz(__ldg(B.vel_b + j)), vi);
-        sum = add(sum, scale_r(scale(m / __ldg(B.rho + j), vd), w));
-    });
+    struct VR {
+        float4 v;
+        float rho;
+    };
+    for_each_neighbor(
+        B, P, i, pi, [&](uint32_t j) { return VR{__ldg(B.vel_b + j), __ldg(B.rho + j)}; },
+        [&](uint32_t, f3 rv, float, float4, VR d) {
+            float r2 = dot(rv, rv);
+            float r = sqrtf(r2);
+            float w = kernel_w(r, h);
+            f3 vd = sub(xyz(d.v), vi);
+            sum = add(sum, scale_r(scale(m / d.rho, vd), w));
+        });
     f3 vv = add(vi, scale(P.visc, sum));
     f3 g = {P.gx, P.gy, P.gz};
     f3 vf = add(vv, scale_r(g, P.dt));
@@ -217,19 +301,21 @@ __global__ void __launch_bounds__(kBlock) k_density_source(Bufs B) {
     const DevParams& P = B.P[s];
     const float m = P.mass, dt = P.dt;
     const f3 pi = xyz(__ldg(B.pos_b + i));
-    const f3 vi = xyz(B.vel_a[i]);
+    const f3 vi = xyz(__ldg(B.vel_a + i));
     float div = 0.0f;
-    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
-        f3 grad = scale(g, rv);
-        f3 vd = sub(vi, xyz(B.vel_a[j]));
-        div += m * dot(vd, grad);
-    });
+    for_each_neighbor(
+        B, P, i, pi, [&](uint32_t j) { return __ldg(B.vel_a + j); },
+        [&](uint32_t, f3 rv, float g, float4, float4 vj) {
+            f3 grad = scale(g, rv);
+            f3 vd = sub(vi, xyz(vj));
+            div += m * dot(vd, grad);
+        });
     float rho_i = B.rho[i];
     float source = 0.0f;
     if (dt > kEpsR) source = ((P.rho0 - rho_i) / dt) - div;
     B.src[i] = source;
     B.prs[i] = 0.0f;
-    B.pr[i] = pressure_over_rho2(0.0f, rho_i);
+    B.pos_b[i].w = pressure_over_rho2(0.0f, rho_i);
 }
 
 // ---------------------------------------------------------------------------
@@ -243,13 +329,15 @@ __global__ void __launch_bounds__(kBlock) k_divergence_source(Bufs B, int fixed)
     const float m = P.mass;
     const float4* __restrict__ vel = fixed ? B.vel_b : B.vel_a;
     const f3 pi = xyz(__ldg(B.pos_b + i));
-    const f3 vi = xyz(vel[i]);
+    const f3 vi = xyz(__ldg(vel + i));
     float div = 0.0f;
-    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
-        f3 grad = scale(g, rv);
-        f3 vd = sub(vi, xyz(vel[j]));
-        div += m * dot(vd, grad);
-    });
+    for_each_neighbor(
+        B, P, i, pi, [&](uint32_t j) { return __ldg(vel + j); },
+        [&](uint32_t, f3 rv, float g, float4, float4 vj) {
+            f3 grad = scale(g, rv);
+            f3 vd = sub(vi, xyz(vj));
+            div += m * dot(vd, grad);
+        });
     B.src[i] = -div;
 }
 
@@ -268,14 +356,16 @@ __global__ void __launch_bounds__(kBlock) k_pressure_force(Bufs B, int which) {
     float p_rho_i = 0.0f;
     if (rho_i > kEpsR) p_rho_i = p_i / (rho_i * rho_i);
     f3 acc = {0.0f, 0.0f, 0.0f};
-    for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
-        float p_rho_j = B.pr[j];
-        if (p_rho_j == p_rho_j) {
-            f3 grad = scale(g, rv);
-            float term = p_rho_i + p_rho_j;
-            acc = add(acc, scale(m * term, grad));
-        }
-    });
+    for_each_neighbor(
+        B, P, i, pi, [&](uint32_t) { return NoData{}; },
+        [&](uint32_t, f3 rv, float g, float4 qj, NoData) {
+            float p_rho_j = qj.w;  // p_j / rho_j^2, NaN when rho_j <= 1e-6
+            if (p_rho_j == p_rho_j) {
+                f3 grad = scale(g, rv);
+                float term = p_rho_i + p_rho_j;
+                acc = add(acc, scale(m * term, grad));
+            }
+        });
     B.acc[i] = make_float4(-acc.x, -acc.y, -acc.z, 0.0f);
 }
 
@@ -344,11 +434,13 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
         const f3 pi = xyz(__ldg(B.pos_b + i));
         const f3 ai = xyz(B.acc[i]);
         float sum_ap = 0.0f;
-        for_each_neighbor(B, P, i, pi, [&](uint32_t j, f3 rv, float g) {
-            f3 grad = scale(g, rv);
-            f3 ad = sub(ai, xyz(B.acc[j]));
-            sum_ap += m * dot(ad, grad);
-        });
+        for_each_neighbor(
+            B, P, i, pi, [&](uint32_t j) { return __ldg(B.acc + j); },
+            [&](uint32_t, f3 rv, float g, float4, float4 aj) {
+                f3 grad = scale(g, rv);
+                f3 ad = sub(ai, xyz(aj));
+                sum_ap += m * dot(ad, grad);
+            });
         const float alpha_i = B.alpha[i], rho_i = B.rho[i], s_i = B.src[i], p_i = B.prs[i];
         float ap_i = dt * sum_ap;
         float error = s_i - ap_i;
@@ -362,7 +454,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
                 B.prs[i] = p_new;
             }
         }
-        B.pr[i] = pressure_over_rho2(p_new, rho_i);
+        B.pos_b[i].w = pressure_over_rho2(p_new, rho_i);
         if (control && P.solver == 1u) {
             float e = which == 1 ? -error : -(dt * error);
             e_sum_in = e > 0.0f ? (double)e : 0.0;

@@ -176,7 +176,7 @@ typedef struct fe_stats {
  * per particle (x, y, z, w) like the reference's vec4 buffers. */
 typedef enum fe_field {
     FE_FIELD_POSITION_A = 0,    /* float4[N]                                 */
-    FE_FIELD_POSITION_B = 1,    /* float4[N] (sorted copy)                   */
+    FE_FIELD_POSITION_B = 1,    /* float4[N] (sorted copy; w reads as 1)     */
     FE_FIELD_VELOCITY_A = 2,    /* float4[N]                                 */
     FE_FIELD_VELOCITY_B = 3,    /* float4[N]                                 */
     FE_FIELD_DENSITY = 4,       /* float[N]                                  */
