@@ -471,23 +471,30 @@ fe_status run_refresh_pr(fe_ctx* c) {
     return FE_OK;
 }
 
-size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem) {
+// Device location of a field: base pointer, element size and the distance
+// between consecutive elements (position_b and the pressure acceleration are
+// interleaved in 32-byte records).  Returns the host-side byte count.
+size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_t* pitch) {
+    *pitch = 0;
+    size_t n = c->n;
     switch (f) {
-        case FE_FIELD_POSITION_A: *dptr = c->B.pos_a; *elem = 16; return (size_t)c->n * 16;
-        case FE_FIELD_POSITION_B: *dptr = c->B.pos_b; *elem = 16; return (size_t)c->n * 16;
-        case FE_FIELD_VELOCITY_A: *dptr = c->B.vel_a; *elem = 16; return (size_t)c->n * 16;
-        case FE_FIELD_VELOCITY_B: *dptr = c->B.vel_b; *elem = 16; return (size_t)c->n * 16;
-        case FE_FIELD_DENSITY: *dptr = c->B.rho; *elem = 4; return (size_t)c->n * 4;
-        case FE_FIELD_FACTOR: *dptr = c->B.alpha; *elem = 4; return (size_t)c->n * 4;
-        case FE_FIELD_SOURCE_TERM: *dptr = c->B.src; *elem = 4; return (size_t)c->n * 4;
-        case FE_FIELD_PRESSURE: *dptr = c->B.prs; *elem = 4; return (size_t)c->n * 4;
-        case FE_FIELD_PRESSURE_ACCEL: *dptr = c->B.acc; *elem = 16; return (size_t)c->n * 16;
-        case FE_FIELD_ENTRY_HASH: *dptr = c->B.keys; *elem = 4; return (size_t)c->T * 4;
-        case FE_FIELD_ENTRY_INDEX: *dptr = c->B.vals; *elem = 4; return (size_t)c->T * 4;
-        case FE_FIELD_GRID_START: *dptr = c->B.cells; *elem = 8; return (size_t)c->T * 4;
-        case FE_FIELD_STATS: *dptr = c->B.S; *elem = 4; return 12;
+        case FE_FIELD_POSITION_A: *dptr = c->B.pos_a; *elem = 16; break;
+        case FE_FIELD_POSITION_B: *dptr = c->B.pos_b; *elem = 16; break;
+        case FE_FIELD_VELOCITY_A: *dptr = c->B.vel_a; *elem = 16; break;
+        case FE_FIELD_VELOCITY_B: *dptr = c->B.vel_b; *elem = 16; break;
+        case FE_FIELD_DENSITY: *dptr = c->B.rho; *elem = 4; break;
+        case FE_FIELD_FACTOR: *dptr = c->B.alpha; *elem = 4; break;
+        case FE_FIELD_SOURCE_TERM: *dptr = c->B.src; *elem = 4; break;
+        case FE_FIELD_PRESSURE: *dptr = c->B.prs; *elem = 4; break;
+        case FE_FIELD_PRESSURE_ACCEL: *dptr = c->B.rec + 1; *elem = 16; *pitch = 32; break;
+        case FE_FIELD_ENTRY_HASH: *dptr = c->B.keys; *elem = 4; n = c->T; break;
+        case FE_FIELD_ENTRY_INDEX: *dptr = c->B.vals; *elem = 4; n = c->T; break;
+        case FE_FIELD_GRID_START: *dptr = c->B.cells; *elem = 4; *pitch = 8; n = c->T; break;
+        case FE_FIELD_STATS: *dptr = c->B.S; *elem = 4; n = 3; break;
         default: return 0;
     }
+    if (*pitch == 0) *pitch = *elem;
+    return n * *elem;
 }
 
 uint64_t graph_key(const fe_ctx* c, uint32_t n_substeps, bool init) {
@@ -700,8 +707,9 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
     uint4* chunks_d = nullptr;
     const size_t scratch_words = radix_scratch_words(n, c->key_bits);
     if ((s = dev_alloc(c, &B.pos_a, n)) || (s = dev_alloc(c, &B.pos_b, n)) ||
+        (s = dev_alloc(c, &B.rec, 2 * (size_t)n)) ||
         (s = dev_alloc(c, &B.vel_a, n)) || (s = dev_alloc(c, &B.vel_b, n)) ||
-        (s = dev_alloc(c, &B.acc, n)) || (s = dev_alloc(c, &B.rho, n)) ||
+        (s = dev_alloc(c, &B.rho, n)) ||
         (s = dev_alloc(c, &B.alpha, n)) || (s = dev_alloc(c, &B.src, n)) ||
         (s = dev_alloc(c, &B.prs, n)) || (s = dev_alloc(c, &B.prs_tmp, n)) ||
         (s = dev_alloc(c, &B.keys, c->T)) ||
@@ -734,8 +742,9 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
                             : make_float4(0, 0, 0, 0);
         FE_CUDA(cudaMemcpy(B.vel_a, h4.data(), (size_t)n * 16, cudaMemcpyHostToDevice));
         FE_CUDA(cudaMemcpy(chunks_d, hc.data(), sizeof(uint4) * nchunks, cudaMemcpyHostToDevice));
-        for (void* p : {(void*)B.pos_b, (void*)B.vel_b, (void*)B.acc})
-            FE_CUDA(cudaMemset(p, 0, (size_t)n * 16));
+        FE_CUDA(cudaMemset(B.rec, 0, (size_t)n * 32));
+        FE_CUDA(cudaMemset(B.pos_b, 0, (size_t)n * 16));
+        FE_CUDA(cudaMemset(B.vel_b, 0, (size_t)n * 16));
         for (void* p : {(void*)B.rho, (void*)B.alpha, (void*)B.src, (void*)B.prs,
                         (void*)B.prs_tmp, (void*)B.nbr_count})
             FE_CUDA(cudaMemset(p, 0, (size_t)n * 4));
@@ -836,14 +845,18 @@ fe_status fe_upload(fe_ctx* c, fe_field f, const void* src, size_t bytes) {
         return FE_ERR_INVALID_ARGUMENT;
     }
     void* d;
-    size_t elem;
-    size_t need = field_bytes(c, f, &d, &elem);
+    size_t elem, pitch;
+    size_t need = field_bytes(c, f, &d, &elem, &pitch);
     if (need == 0 || bytes != need || f == FE_FIELD_STATS || f == FE_FIELD_GRID_START) {
         set_error("field %d: expected %zu bytes, got %zu (or read-only field)", (int)f, need, bytes);
         return FE_ERR_INVALID_ARGUMENT;
     }
     FE_CUDA(cudaSetDevice(c->device));
-    FE_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    FE_CUDA(cudaMemcpy2DAsync(d, pitch, src, elem, elem, need / elem, cudaMemcpyHostToDevice,
+                              c->stream));
+    if (f == FE_FIELD_POSITION_B)  // keep pressure_update's copy in the records
+        FE_CUDA(cudaMemcpy2DAsync(c->B.rec, 32, src, 16, 16, c->n, cudaMemcpyHostToDevice,
+                                  c->stream));
     // pos_b.w caches p / rho^2 for pressure_force.
     if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY || f == FE_FIELD_POSITION_B)
         return run_refresh_pr(c);
@@ -856,18 +869,15 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
         return FE_ERR_INVALID_ARGUMENT;
     }
     void* d;
-    size_t elem;
-    size_t need = field_bytes(c, f, &d, &elem);
+    size_t elem, pitch;
+    size_t need = field_bytes(c, f, &d, &elem, &pitch);
     if (need == 0 || bytes != need) {
         set_error("field %d: expected %zu bytes, got %zu", (int)f, need, bytes);
         return FE_ERR_INVALID_ARGUMENT;
     }
     FE_CUDA(cudaSetDevice(c->device));
-    if (f == FE_FIELD_GRID_START) {
-        FE_CUDA(cudaMemcpy2DAsync(dst, 4, d, 8, 4, c->T, cudaMemcpyDeviceToHost, c->stream));
-    } else {
-        FE_CUDA(cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, c->stream));
-    }
+    FE_CUDA(cudaMemcpy2DAsync(dst, elem, d, pitch, elem, need / elem, cudaMemcpyDeviceToHost,
+                              c->stream));
     FE_CUDA(cudaStreamSynchronize(c->stream));
     if (f == FE_FIELD_POSITION_B) {
         // The device keeps p / rho^2 in w; the reference's position_b.w is the

@@ -37,6 +37,12 @@ __device__ __forceinline__ uint32_t cell_hash(int cx, int cy, int cz, uint32_t t
             ((uint32_t)cz * 83492791u)) % table;
 }
 
+// get_cell_hash for a power-of-two table: x % T == x & (T - 1).
+__device__ __forceinline__ uint32_t cell_hash_pow2(int cx, int cy, int cz, uint32_t mask) {
+    return (((uint32_t)cx * 73856093u) ^ ((uint32_t)cy * 19349663u) ^
+            ((uint32_t)cz * 83492791u)) & mask;
+}
+
 // ivec3(floor(p / h)): IEEE division, floor, saturating conversion (NaN -> 0).
 __device__ __forceinline__ int cell_coord(float p, float h) {
     return __float2int_rz(floorf(p / h));
@@ -82,6 +88,24 @@ __device__ __forceinline__ float pressure_over_rho2(float p, float rho) {
 }
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// position_b and pressure acceleration of particle i (see Bufs).
+__device__ __forceinline__ float4* posb(const Bufs& B, uint32_t i) { return B.pos_b + i; }
+__device__ __forceinline__ float4* rec_pos(const Bufs& B, uint32_t i) {
+    return B.rec + 2 * (size_t)i;
+}
+__device__ __forceinline__ float4* accp(const Bufs& B, uint32_t i) {
+    return B.rec + 2 * (size_t)i + 1;
+}
+
+// Both halves of particle j's record in one 256-bit read-only load.
+__device__ __forceinline__ void ld_record(const Bufs& B, uint32_t j, float4& pos, float4& acc) {
+    const float4* p = B.rec + 2 * (size_t)j;
+    asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(pos.x), "=f"(pos.y), "=f"(pos.z), "=f"(pos.w), "=f"(acc.x), "=f"(acc.y),
+                   "=f"(acc.z), "=f"(acc.w)
+                 : "l"(p));
+}
 
 // Fixed-order FP64 sum of one value per thread of a 256-thread block:
 // warp halving tree (lane l + lane l^m, m = 16..1), then the 8 warp sums in a

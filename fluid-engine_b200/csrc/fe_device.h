@@ -72,7 +72,13 @@ enum Ticket : int { kTicketStats = 0, kTicketSolve = 1, kTicketHist = 2 };
 
 // Kernel-side view of every buffer of a context (passed by value).
 struct Bufs {
-    float4 *pos_a, *pos_b, *vel_a, *vel_b, *acc;  // pos_b.w = p / rho^2 (NaN: rho <= 1e-6)
+    float4 *pos_a, *vel_a, *vel_b;
+    // position_b; w holds p / rho^2 (NaN when rho <= 1e-6) for pressure_force.
+    float4* pos_b;
+    // 32-byte record per particle: rec[2i] = copy of position_b (xyz),
+    // rec[2i+1] = pressure acceleration.  pressure_update fetches both halves
+    // of a neighbour with one 256-bit load.
+    float4* rec;
     float *rho, *alpha, *src, *prs, *prs_tmp;
     uint32_t *keys, *vals;      // grid_entries (hash, index), T_total
     uint2* cells;               // {start, end} per table slot, T_total

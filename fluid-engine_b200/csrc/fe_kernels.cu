@@ -41,13 +41,13 @@ __device__ __forceinline__ void walk(const Bufs& B, const DevParams& P, f3 pi, F
         for (int y = -1; y <= 1; ++y)
             for (int x = -1; x <= 1; ++x) {
                 uint32_t k = P.table_base +
-                             cell_hash((int)((uint32_t)cx + (uint32_t)x),
-                                       (int)((uint32_t)cy + (uint32_t)y),
-                                       (int)((uint32_t)cz + (uint32_t)z), P.T);
+                             cell_hash_pow2((int)((uint32_t)cx + (uint32_t)x),
+                                            (int)((uint32_t)cy + (uint32_t)y),
+                                            (int)((uint32_t)cz + (uint32_t)z), P.T - 1u);
                 uint2 cell = B.cells[k];
                 if (cell.x == kEmpty) continue;
                 for (uint32_t j = cell.x; j < cell.y; ++j) {
-                    f3 rv = sub(pi, xyz(__ldg(B.pos_b + j)));
+                    f3 rv = sub(pi, xyz(__ldg(posb(B, j))));
                     float r2 = dot(rv, rv);
                     if (r2 > h2) continue;
                     f(j, rv, r2);
@@ -90,8 +90,8 @@ __device__ __forceinline__ void for_each_neighbor(const Bufs& B, const DevParams
             uint2 v1 = ld_list(e + (k + 1) * stride, pol);
             uint2 v2 = ld_list(e + (k + 2) * stride, pol);
             uint2 v3 = ld_list(e + (k + 3) * stride, pol);
-            float4 q0 = __ldg(B.pos_b + v0.x), q1 = __ldg(B.pos_b + v1.x);
-            float4 q2 = __ldg(B.pos_b + v2.x), q3 = __ldg(B.pos_b + v3.x);
+            float4 q0 = __ldg(posb(B, v0.x)), q1 = __ldg(posb(B, v1.x));
+            float4 q2 = __ldg(posb(B, v2.x)), q3 = __ldg(posb(B, v3.x));
             auto d0 = gather(v0.x);
             auto d1 = gather(v1.x);
             auto d2 = gather(v2.x);
@@ -103,19 +103,60 @@ __device__ __forceinline__ void for_each_neighbor(const Bufs& B, const DevParams
         }
         for (; k < cnt; ++k) {
             uint2 v = ld_list(e + k * stride, pol);
-            float4 q = __ldg(B.pos_b + v.x);
+            float4 q = __ldg(posb(B, v.x));
             f(v.x, sub(pi, xyz(q)), __uint_as_float(v.y), q, gather(v.x));
         }
     } else {
         const float h = P.h;
         walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
             float r = sqrtf(r2);
-            if (r > kEpsR) f(j, rv, kernel_grad_scale(r, h), __ldg(B.pos_b + j), gather(j));
+            if (r > kEpsR) f(j, rv, kernel_grad_scale(r, h), __ldg(posb(B, j)), gather(j));
         });
     }
 }
 
 struct NoData {};
+
+// As for_each_neighbor, for pressure_update: f(r_vec, grad_scale, acc_j),
+// with position and acceleration of j fetched by one 256-bit load.
+template <class F>
+__device__ __forceinline__ void for_each_neighbor_record(const Bufs& B, const DevParams& P,
+                                                         uint32_t i, f3 pi, F&& f) {
+    const uint32_t cnt = B.nbr_count[i];
+    if (cnt <= kNbrCap) {
+        const uint2* e = B.nbr + i;
+        const size_t stride = B.n_total;
+        const uint64_t pol = evict_first_policy();
+        uint32_t k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+            uint2 v0 = ld_list(e + (k + 0) * stride, pol);
+            uint2 v1 = ld_list(e + (k + 1) * stride, pol);
+            uint2 v2 = ld_list(e + (k + 2) * stride, pol);
+            uint2 v3 = ld_list(e + (k + 3) * stride, pol);
+            float4 q0, a0, q1, a1, q2, a2, q3, a3;
+            ld_record(B, v0.x, q0, a0);
+            ld_record(B, v1.x, q1, a1);
+            ld_record(B, v2.x, q2, a2);
+            ld_record(B, v3.x, q3, a3);
+            f(sub(pi, xyz(q0)), __uint_as_float(v0.y), a0);
+            f(sub(pi, xyz(q1)), __uint_as_float(v1.y), a1);
+            f(sub(pi, xyz(q2)), __uint_as_float(v2.y), a2);
+            f(sub(pi, xyz(q3)), __uint_as_float(v3.y), a3);
+        }
+        for (; k < cnt; ++k) {
+            uint2 v = ld_list(e + k * stride, pol);
+            float4 q, a;
+            ld_record(B, v.x, q, a);
+            f(sub(pi, xyz(q)), __uint_as_float(v.y), a);
+        }
+    } else {
+        const float h = P.h;
+        walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
+            float r = sqrtf(r2);
+            if (r > kEpsR) f(rv, kernel_grad_scale(r, h), __ldg(accp(B, j)));
+        });
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Neighbour search: spatial_hash.comp, grid_offsets.comp, reorder.comp.
@@ -139,8 +180,8 @@ __global__ void __launch_bounds__(kBlock) k_hash(Bufs B) {
     const DevParams& P = B.P[s];
     float4 p = __ldg(B.pos_a + i);
     const float h = P.h;
-    B.keys[i] = P.table_base + cell_hash(cell_coord(p.x, h), cell_coord(p.y, h),
-                                         cell_coord(p.z, h), P.T);
+    B.keys[i] = P.table_base + cell_hash_pow2(cell_coord(p.x, h), cell_coord(p.y, h),
+                                              cell_coord(p.z, h), P.T - 1u);
     B.vals[i] = i;
 }
 
@@ -169,8 +210,9 @@ __global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) 
     // pos_b.w holds p / rho^2 of slot i (pressures and densities are not
     // permuted here), so it is carried over.
     float4 p = __ldg(B.pos_a + src);
-    p.w = B.pos_b[i].w;
-    B.pos_b[i] = p;
+    p.w = posb(B, i)->w;
+    *posb(B, i) = p;
+    *rec_pos(B, i) = p;
     B.vel_b[i] = __ldg(B.vel_a + src);
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
 }
@@ -182,14 +224,14 @@ __global__ void __launch_bounds__(kBlock) k_take_pressure(Bufs B) {
     if (i >= B.n_total) return;
     float p = B.prs_tmp[i];
     B.prs[i] = p;
-    B.pos_b[i].w = pressure_over_rho2(p, B.rho[i]);
+    posb(B, i)->w = pressure_over_rho2(p, B.rho[i]);
 }
 
 // pr = p / rho^2 for all particles (after a host upload of p or rho).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
-    B.pos_b[i].w = pressure_over_rho2(B.prs[i], B.rho[i]);
+    posb(B, i)->w = pressure_over_rho2(B.prs[i], B.rho[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -227,13 +269,13 @@ __device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, ui
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_density_alpha(Bufs B) {
+__global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
     __shared__ uint32_t s_cand[kStage][kBlock];
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
-    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 pi = xyz(__ldg(posb(B, i)));
     uint2* out = B.nbr + i;
     const uint32_t stride = B.n_total;
     const int t = threadIdx.x;
@@ -248,7 +290,7 @@ __global__ void __launch_bounds__(kBlock) k_density_alpha(Bufs B) {
         // Phase 2: the recorded candidates, same order.
         for (uint32_t k = 0; k < n1; ++k) {
             uint32_t j = s_cand[k][t];
-            f3 rv = sub(pi, xyz(__ldg(B.pos_b + j)));
+            f3 rv = sub(pi, xyz(__ldg(posb(B, j))));
             density_term(a, m, h, j, rv, dot(rv, rv), out, stride);
         }
     } else {
@@ -258,19 +300,19 @@ __global__ void __launch_bounds__(kBlock) k_density_alpha(Bufs B) {
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
     B.alpha[i] = al > kEpsR ? al : 0.0f;
     B.nbr_count[i] = a.cnt;
-    B.pos_b[i].w = pressure_over_rho2(B.prs[i], a.density);
+    posb(B, i)->w = pressure_over_rho2(B.prs[i], a.density);
     if (a.cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
 }
 
 // ---------------------------------------------------------------------------
 // viscosity.comp:17-66: velocity_b in, velocity_a out.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_viscosity(Bufs B) {
+__global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
-    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(B.vel_b + i));
     f3 sum = {0.0f, 0.0f, 0.0f};
     struct VR {
@@ -295,12 +337,12 @@ __global__ void __launch_bounds__(kBlock) k_viscosity(Bufs B) {
 // ---------------------------------------------------------------------------
 // density_source_term.comp:16-74 (velocities = velocity_a).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_density_source(Bufs B) {
+__global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     const float m = P.mass, dt = P.dt;
-    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(B.vel_a + i));
     float div = 0.0f;
     for_each_neighbor(
@@ -315,20 +357,20 @@ __global__ void __launch_bounds__(kBlock) k_density_source(Bufs B) {
     if (dt > kEpsR) source = ((P.rho0 - rho_i) / dt) - div;
     B.src[i] = source;
     B.prs[i] = 0.0f;
-    B.pos_b[i].w = pressure_over_rho2(0.0f, rho_i);
+    posb(B, i)->w = pressure_over_rho2(0.0f, rho_i);
 }
 
 // ---------------------------------------------------------------------------
 // divergence_source_term.comp:14-61 (velocities = velocity_a in REFERENCE
 // mode, velocity_b in FIXED mode).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_divergence_source(Bufs B, int fixed) {
+__global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fixed) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     const float m = P.mass;
     const float4* __restrict__ vel = fixed ? B.vel_b : B.vel_a;
-    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(vel + i));
     float div = 0.0f;
     for_each_neighbor(
@@ -345,13 +387,13 @@ __global__ void __launch_bounds__(kBlock) k_divergence_source(Bufs B, int fixed)
 // pressure_force.comp:15-78.  pr[j] = p_j / rho_j^2 (NaN when rho_j <= 1e-6)
 // is maintained by every pass that writes p or rho.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_pressure_force(Bufs B, int which) {
+__global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     if (which >= 0 && B.S[s].solve[which].done) return;
     const DevParams& P = B.P[s];
     const float m = P.mass;
-    const f3 pi = xyz(__ldg(B.pos_b + i));
+    const f3 pi = xyz(__ldg(posb(B, i)));
     const float rho_i = B.rho[i], p_i = B.prs[i];
     float p_rho_i = 0.0f;
     if (rho_i > kEpsR) p_rho_i = p_i / (rho_i * rho_i);
@@ -366,7 +408,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_force(Bufs B, int which) {
                 acc = add(acc, scale(m * term, grad));
             }
         });
-    B.acc[i] = make_float4(-acc.x, -acc.y, -acc.z, 0.0f);
+    *accp(B, i) = make_float4(-acc.x, -acc.y, -acc.z, 0.0f);
 }
 
 // ---------------------------------------------------------------------------
@@ -431,16 +473,14 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
     double e_sum_in = 0.0;
     if (valid && !skip) {
         const float m = P.mass, dt = P.dt, omega = P.omega;
-        const f3 pi = xyz(__ldg(B.pos_b + i));
-        const f3 ai = xyz(B.acc[i]);
+        const f3 pi = xyz(__ldg(posb(B, i)));
+        const f3 ai = xyz(*accp(B, i));
         float sum_ap = 0.0f;
-        for_each_neighbor(
-            B, P, i, pi, [&](uint32_t j) { return __ldg(B.acc + j); },
-            [&](uint32_t, f3 rv, float g, float4, float4 aj) {
-                f3 grad = scale(g, rv);
-                f3 ad = sub(ai, xyz(aj));
-                sum_ap += m * dot(ad, grad);
-            });
+        for_each_neighbor_record(B, P, i, pi, [&](f3 rv, float g, float4 aj) {
+            f3 grad = scale(g, rv);
+            f3 ad = sub(ai, xyz(aj));
+            sum_ap += m * dot(ad, grad);
+        });
         const float alpha_i = B.alpha[i], rho_i = B.rho[i], s_i = B.src[i], p_i = B.prs[i];
         float ap_i = dt * sum_ap;
         float error = s_i - ap_i;
@@ -454,7 +494,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
                 B.prs[i] = p_new;
             }
         }
-        B.pos_b[i].w = pressure_over_rho2(p_new, rho_i);
+        posb(B, i)->w = pressure_over_rho2(p_new, rho_i);
         if (control && P.solver == 1u) {
             float e = which == 1 ? -error : -(dt * error);
             e_sum_in = e > 0.0f ? (double)e : 0.0;
@@ -536,9 +576,9 @@ __global__ void __launch_bounds__(kBlock) k_pressure_integration(Bufs B) {
     const DevParams& P = B.P[s];
     const float dt = P.dt, r = P.radius;
     const float rest = 0.5f, fric = 0.95f, eps = 0.001f;
-    f3 pos = xyz(__ldg(B.pos_b + i));
+    f3 pos = xyz(__ldg(posb(B, i)));
     f3 vel = xyz(B.vel_a[i]);
-    f3 ap = xyz(B.acc[i]);
+    f3 ap = xyz(*accp(B, i));
     f3 nv = add(vel, scale_r(ap, dt));
     f3 np = add(pos, scale_r(nv, dt));
     if (np.y < P.bminy + r) {
@@ -566,7 +606,7 @@ __global__ void __launch_bounds__(kBlock) k_divergence_integration(Bufs B, int f
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     float4* vel = fixed ? B.vel_b : B.vel_a;
-    f3 nv = add(xyz(vel[i]), scale_r(xyz(B.acc[i]), P.dt));
+    f3 nv = add(xyz(vel[i]), scale_r(xyz(*accp(B, i)), P.dt));
     vel[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
 }
 
