@@ -1,0 +1,58 @@
+// fe_mlp.h — tensor-core MLP of the learned warm start (fe_mlp.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace fe {
+namespace mlp {
+
+// Parameter layout (FP32 master and gradients, in this order):
+//   w1 [64][16] (input columns 12..15 stay zero), w2 [64][64], w3 [2][64],
+//   b1 [64], b2 [64], b3 [2].
+// The BF16 weight copy holds w1, w2, w3 in the same order.
+constexpr uint32_t kW1 = 64 * 16, kW2 = 64 * 64, kW3 = 2 * 64;
+constexpr uint32_t kWeights = kW1 + kW2 + kW3;         // 5248
+constexpr uint32_t kParams = kWeights + 64 + 64 + 2;   // 5378
+constexpr uint32_t kFeatures = 12;
+
+struct Params {
+    const __nv_bfloat16 *w1, *w2, *w3;
+    const float *b1, *b2, *b3;
+};
+
+struct Grads {
+    float *w1, *w2, *w3, *b1, *b2, *b3;
+    float* loss;
+};
+
+inline Params params_from(const __nv_bfloat16* wbf16, const float* master) {
+    return Params{wbf16, wbf16 + kW1, wbf16 + kW1 + kW2, master + kWeights,
+                  master + kWeights + 64, master + kWeights + 128};
+}
+inline Grads grads_from(float* g, float* loss) {
+    return Grads{g, g + kW1, g + kW1 + kW2, g + kWeights, g + kWeights + 64, g + kWeights + 128,
+                 loss};
+}
+
+size_t infer_smem_bytes();
+size_t train_smem_bytes();
+
+// out[i][0..1] for the BF16 rows X[i][0..15], i < n.
+cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t n,
+                  uint32_t* error_flags, cudaStream_t stream, int num_sms);
+
+// Adds d(loss)/d(params) of the mean squared error over the n samples to G
+// (G must be zeroed by the caller; Adam zeroes it after each step).
+cudaError_t train_grads(const Params& P, const __nv_bfloat16* X, const float* Y, uint32_t n,
+                        const Grads& G, uint32_t* error_flags, cudaStream_t stream, int num_sms);
+
+cudaError_t adam(float* master, float* grad, float* m, float* v, __nv_bfloat16* bf16_copy,
+                 uint32_t count, uint32_t bf16_count, float lr, float beta1, float beta2, float eps,
+                 uint32_t step, float weight_decay, cudaStream_t stream);
+
+}  // namespace mlp
+}  // namespace fe

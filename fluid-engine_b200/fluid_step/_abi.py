@@ -258,7 +258,21 @@ SIGNATURES = {
     "fe_sort_pairs": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p]),
     "fe_sort_pairs_host": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int]),
     "fe_sort_pairs_noalloc": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p]),
+    "fe_model_create": (c_int, [c_uint32, c_int, POINTER(c_void_p)]),
+    "fe_model_destroy": (c_int, [c_void_p]),
+    "fe_model_set_parameters": (c_int, [c_void_p, c_void_p, c_size_t]),
+    "fe_model_get_parameters": (c_int, [c_void_p, c_void_p, c_size_t]),
+    "fe_model_set_normalization": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fe_model_get_normalization": (c_int, [c_void_p, c_void_p]),
+    "fe_model_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+    "fe_model_gradients": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
+    "fe_model_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_float, c_float,
+                                    c_void_p, c_void_p]),
+    "fe_model_read_flags": (c_int, [c_void_p, POINTER(c_uint32)]),
 }
+
+FE_MODEL_PARAMS = 5378
+FE_MODEL_FEATURES = 12
 
 FE_SORT_NOALLOC_MAX_PAIRS = 1 << 20
 

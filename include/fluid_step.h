@@ -329,6 +329,46 @@ FE_API fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
 FE_API fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* values, uint32_t n,
                              uint32_t key_bits, int algorithm);
 
+/* ------------------------------------------------------------------------- */
+/* Learned warm start (no reference counterpart)                             */
+/* ------------------------------------------------------------------------- */
+/* A per-particle MLP 12 -> 64 -> 64 -> 2 (SiLU; BF16 weights, FP32
+ * accumulation on the tensor cores) maps neighbourhood features to the
+ * initial pressure of the density and divergence solves.  Parameter vector
+ * (FE_MODEL_PARAMS floats): w1[64][16] (input columns 12..15 unused),
+ * w2[64][64], w3[2][64], b1[64], b2[64], b3[2].  Features and targets are
+ * standardised with the model's normalisation before the network. */
+#define FE_MODEL_PARAMS 5378u
+#define FE_MODEL_FEATURES 12u
+typedef struct fe_model fe_model;
+
+/* Random initialisation (seeded) on `device`. */
+FE_API fe_status fe_model_create(uint32_t seed, int device, fe_model** out);
+FE_API fe_status fe_model_destroy(fe_model* model);
+FE_API fe_status fe_model_set_parameters(fe_model* model, const float* params, size_t count);
+FE_API fe_status fe_model_get_parameters(const fe_model* model, float* params, size_t count);
+/* x_mean/x_std: 12 floats; y_mean/y_std: 2 floats. */
+FE_API fe_status fe_model_set_normalization(fe_model* model, const float* x_mean,
+                                            const float* x_std, const float* y_mean,
+                                            const float* y_std);
+/* 32 floats: x mean[12], x std[12], y mean[2], y std[2], 4 unused. */
+FE_API fe_status fe_model_get_normalization(const fe_model* model, float* out32);
+/* d_y[n][2] = model(d_x[n][12]) in target units (device pointers). */
+FE_API fe_status fe_model_forward(fe_model* model, const float* d_x, float* d_y, uint32_t n,
+                                  void* stream);
+/* Gradients of the mean squared error (standardised targets) over the n
+ * samples, copied to h_grads (FE_MODEL_PARAMS floats) and the summed squared
+ * error to h_loss (either may be NULL).  Synchronous; no update. */
+FE_API fe_status fe_model_gradients(fe_model* model, const float* d_x, const float* d_y,
+                                    uint32_t n, float* h_grads, float* h_loss);
+/* One Adam step (beta 0.9 / 0.999) on the minibatch d_x[n][12], d_y[n][2].
+ * When h_loss is given, waits and stores the mean squared error per sample. */
+FE_API fe_status fe_model_train_step(fe_model* model, const float* d_x, const float* d_y,
+                                     uint32_t n, float lr, float weight_decay, void* stream,
+                                     float* h_loss);
+/* Device error word of the model's kernels (FE_STATS_* bits). */
+FE_API fe_status fe_model_read_flags(fe_model* model, uint32_t* flags);
+
 /* Radix sort that allocates nothing.  No counterpart in the reference: it is
  * for callers that cannot let a library allocate device memory — a frame
  * loop that must not stall (cudaMalloc/cudaFree synchronise the device),
