@@ -26,6 +26,8 @@
 #include "fe_device.h"
 #include "fe_error.h"
 #include "fe_kernels.h"
+#include "fe_mlp.h"
+#include "fe_model.h"
 #include "fe_sort.h"
 
 using namespace fe;
@@ -173,10 +175,6 @@ fe_status validate(const fe_params* p) {
         set_error("enum field out of range");
         return FE_ERR_INVALID_ARGUMENT;
     }
-    if (p->warm_start == FE_WARM_LEARNED) {
-        set_error("learned warm start needs a trained model (not loaded)");
-        return FE_ERR_UNSUPPORTED;
-    }
     if (p->solver == FE_SOLVER_TOLERANCE &&
         (p->max_iterations == 0 || p->min_iterations > p->max_iterations)) {
         set_error("tolerance solver needs 0 < max_iterations and min <= max");
@@ -268,6 +266,13 @@ struct fe_ctx {
     std::vector<GraphEntry> graphs;
     SceneState* h_state = nullptr;   // pinned
     GlobalState* h_global = nullptr; // pinned
+    // learned warm start / capture
+    fe_model* model = nullptr;       // attached, not owned
+    LearnArgs L{};
+    bool capture = false;
+
+    bool learned() const { return params[0].warm_start == FE_WARM_LEARNED && model != nullptr; }
+    bool carries() const { return L.carry != nullptr && (learned() || capture); }
 
     uint32_t sort_algorithm() const { return params[0].sort_algorithm; }
     bool fixed_mode() const { return params[0].mode == FE_MODE_FIXED; }
@@ -350,6 +355,10 @@ fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
     REC(R.k(k_offsets, flat_grid(c->n), dim3(kBlock), B));
     REC(R.k(k_reorder, flat_grid(c->n), dim3(kBlock), B, c->fixed_mode() ? 1 : 0));
     if (c->fixed_mode()) REC(R.k(k_take_pressure, flat_grid(c->n), dim3(kBlock), B));
+    if (c->carries()) {
+        REC(R.k(k_carry_gather, flat_grid(c->n), dim3(kBlock), B, c->L));
+        REC(R.k(k_carry_take, flat_grid(c->n), dim3(kBlock), B, c->L));
+    }
     return FE_OK;
 }
 
@@ -407,6 +416,22 @@ fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
     return FE_OK;
 }
 
+// Network inference on the feature rows (tensor-core kernel of fe_mlp.cu).
+fe_status rec_mlp(fe_ctx* c, Recorder& R) {
+    mlp::KernelLaunch KL;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    REC(mlp::infer_launch(c->n, sms, &KL));
+    mlp::Params P = c->model->params();
+    const __nv_bfloat16* X = static_cast<const __nv_bfloat16*>(c->L.xb);
+    float* out = c->L.out;
+    uint32_t n = c->n;
+    uint32_t* flags = &c->B.G->flags;
+    void* args[] = {&P, &X, &out, &n, &flags};
+    REC(R.launch(KL.func, KL.grid, KL.block, KL.smem, args));
+    return FE_OK;
+}
+
 // One substep of Renderer::step (renderer/mod.rs:289-337).
 fe_status rec_substep(fe_ctx* c, Recorder& R) {
     Bufs B = c->B;
@@ -414,12 +439,24 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
     fe_status s;
     if ((s = rec_simple(c, R, k_viscosity))) return s;
     if ((s = rec_simple(c, R, k_density_source))) return s;
+    if (c->carries()) REC(R.k(k_features, chunk_grid(c), dim3(kBlock), B, c->L, 0));
+    if (c->learned()) {
+        if ((s = rec_mlp(c, R))) return s;
+        REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 0));
+    }
     if ((s = rec_solve(c, R, 0))) return s;
+    if (c->carries()) REC(R.k(k_after_solve, chunk_grid(c), dim3(kBlock), B, c->L, 0));
     if ((s = rec_simple(c, R, k_pressure_integration))) return s;
     if ((s = rec_neighbor_search(c, R))) return s;
     if ((s = rec_simple(c, R, k_density_alpha))) return s;
     REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));
+    if (c->carries()) REC(R.k(k_features, chunk_grid(c), dim3(kBlock), B, c->L, 1));
+    if (c->learned()) {
+        if ((s = rec_mlp(c, R))) return s;
+        REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 1));
+    }
     if ((s = rec_solve(c, R, 1))) return s;
+    if (c->carries()) REC(R.k(k_after_solve, chunk_grid(c), dim3(kBlock), B, c->L, 1));
     REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), B, fixed));
     REC(R.k(k_count_substep, dim3(1), dim3(64), B));
     return FE_OK;
@@ -499,7 +536,8 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
 
 uint64_t graph_key(const fe_ctx* c, uint32_t n_substeps, bool init) {
     return (uint64_t)n_substeps | ((uint64_t)init << 32) | ((uint64_t)c->sort_algorithm() << 33) |
-           ((uint64_t)c->fixed_mode() << 34);
+           ((uint64_t)c->fixed_mode() << 34) | ((uint64_t)c->learned() << 35) |
+           ((uint64_t)c->capture << 36);
 }
 
 fe_status get_graph(fe_ctx* c, uint32_t n_substeps, bool init, cudaGraphExec_t* out) {
@@ -933,6 +971,10 @@ fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out)
         set_error("n_substeps %u above 1024", n_substeps);
         return FE_ERR_CAPACITY;
     }
+    if (c->params[0].warm_start == FE_WARM_LEARNED && !c->model) {
+        set_error("fe_step: warm_start = FE_WARM_LEARNED needs a model (fe_set_model)");
+        return FE_ERR_UNSUPPORTED;
+    }
     const bool init = (flags & FE_STEP_INIT_NS) || !c->initialized;
     if (flags & FE_STEP_NO_GRAPH) {
         Recorder R = eager(c);
@@ -958,6 +1000,115 @@ fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out)
     }
     return FE_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Learned warm start: model attachment and training-data capture.
+// ---------------------------------------------------------------------------
+static fe_status ensure_learn_buffers(fe_ctx* c) {
+    if (c->L.carry) return FE_OK;
+    fe_status s;
+    __nv_bfloat16* xb = nullptr;
+    if ((s = dev_alloc(c, &xb, (size_t)c->n * 16)) || (s = dev_alloc(c, &c->L.out, 2 * (size_t)c->n)) ||
+        (s = dev_alloc(c, &c->L.carry_tmp, c->n)))
+        return s;
+    float4* carry = nullptr;
+    if ((s = dev_alloc(c, &carry, c->n))) return s;
+    c->L.xb = xb;
+    FE_CUDA(cudaMemsetAsync(carry, 0, (size_t)c->n * 16, c->stream));
+    // no capture slot yet: w = all ones
+    FE_CUDA(cudaMemset2DAsync(reinterpret_cast<char*>(carry) + 12, 16, 0xFF, 4, c->n, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    c->L.carry = carry;
+    return FE_OK;
+}
+
+static void drop_graphs(fe_ctx* c) {
+    cudaStreamSynchronize(c->stream);
+    for (auto& g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    c->graphs.clear();
+}
+
+extern "C" {
+
+FE_API fe_status fe_set_model(fe_ctx* c, fe_model* model) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (model && model->device != c->device) {
+        set_error("model lives on device %d, context on %d", model->device, c->device);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    fe_status s = ensure_learn_buffers(c);
+    if (s != FE_OK) return s;
+    drop_graphs(c);  // recorded graphs hold the previous model's pointers
+    c->model = model;
+    c->L.norm = model ? model->norm : nullptr;
+    c->L.learned = model ? 1u : 0u;
+    return FE_OK;
+}
+
+FE_API fe_status fe_capture_begin(fe_ctx* c, uint32_t capacity, uint32_t stride) {
+    if (!c || capacity == 0 || stride == 0) {
+        set_error("capacity and stride must be > 0");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    fe_status s = ensure_learn_buffers(c);
+    if (s != FE_OK) return s;
+    if (c->L.cap_capacity < capacity) {
+        if ((s = dev_alloc(c, &c->L.cap_x, (size_t)capacity * 12)) ||
+            (s = dev_alloc(c, &c->L.cap_y, (size_t)capacity * 2)))
+            return s;
+        if (!c->L.cap_count && (s = dev_alloc(c, &c->L.cap_count, 4))) return s;
+        c->L.cap_capacity = capacity;
+    }
+    FE_CUDA(cudaMemsetAsync(c->L.cap_count, 0, 4, c->stream));
+    drop_graphs(c);
+    c->L.cap_stride = stride;
+    c->L.capture = 1;
+    c->capture = true;
+    return FE_OK;
+}
+
+FE_API fe_status fe_capture_read(fe_ctx* c, float* x, float* y, uint32_t rows, uint32_t* count) {
+    if (!c || !count || (rows && (!x || !y))) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    uint32_t n = 0;
+    if (c->L.cap_count) {
+        FE_CUDA(cudaMemcpyAsync(&n, c->L.cap_count, 4, cudaMemcpyDeviceToHost, c->stream));
+        FE_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    if (n > c->L.cap_capacity) n = c->L.cap_capacity;
+    *count = n;
+    uint32_t k = n < rows ? n : rows;
+    if (k) {
+        FE_CUDA(cudaMemcpy(x, c->L.cap_x, (size_t)k * 12 * 4, cudaMemcpyDeviceToHost));
+        FE_CUDA(cudaMemcpy(y, c->L.cap_y, (size_t)k * 2 * 4, cudaMemcpyDeviceToHost));
+    }
+    return FE_OK;
+}
+
+FE_API fe_status fe_capture_end(fe_ctx* c) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    drop_graphs(c);
+    c->capture = false;
+    c->L.capture = 0;
+    return FE_OK;
+}
+
+}  // extern "C"
 
 // ---------------------------------------------------------------------------
 // Standalone sort (device buffers).  Scratch per device, grown on demand;

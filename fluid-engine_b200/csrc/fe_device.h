@@ -92,4 +92,24 @@ struct Bufs {
     uint32_t n_total, T_total, n_chunks, n_scenes;
 };
 
+// Learned warm start and training-data capture (fe_learned.cu).
+// carry[i] travels with particle i through every re-sort:
+//   x = final pressure of the last density solve, y = of the last
+//   divergence solve, z unused, w = capture slot of the solve in progress
+//   (bits; ~0 none).
+struct LearnArgs {
+    const float* norm;          // model standardisation: x mean[12], std[12], y mean[2], std[2]
+    void* xb;                   // BF16 feature rows [n][16] (network input)
+    float* out;                 // network output [n][2] (standardised)
+    float4* carry;
+    float4* carry_tmp;
+    float* cap_x;               // captured raw features [capacity][12]
+    float* cap_y;               // captured normalised targets [capacity][2]
+    uint32_t* cap_count;
+    uint32_t cap_capacity;
+    uint32_t cap_stride;        // sample one particle in cap_stride (hashed)
+    uint32_t capture;           // 1: record samples this frame
+    uint32_t learned;           // 1: apply the network's pressures
+};
+
 }  // namespace fe

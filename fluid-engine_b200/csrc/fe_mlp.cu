@@ -312,8 +312,8 @@ __global__ void __launch_bounds__(kThreads) k_mlp_infer(Params P, const __nv_bfl
 
 // ---------------------------------------------------------------------------
 // Training step: gradients of the mean squared error over n samples
-// (normalised targets), accumulated into grads (FP32, atomics, one add per
-// parameter per block).  512 TMEM columns, one block per SM (the shared
+// (normalised targets; a NaN target masks that output of the sample),
+// accumulated into grads (FP32, atomics, one add per parameter per block).  512 TMEM columns, one block per SM (the shared
 // memory footprint keeps it so).
 // ---------------------------------------------------------------------------
 struct TrainSmem {
@@ -428,10 +428,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
         if (ok) {
             float v[16];
             tmem_ld16(lane_addr(c_o, 0), v);
+            // A NaN target means "no target for this output" (masked).
             float e0 = 0.0f, e1 = 0.0f;
             if (valid) {
-                e0 = v[0] + S.W.b3[0] - Y[2 * (size_t)g];
-                e1 = v[1] + S.W.b3[1] - Y[2 * (size_t)g + 1];
+                const float y0 = Y[2 * (size_t)g], y1 = Y[2 * (size_t)g + 1];
+                e0 = y0 == y0 ? v[0] + S.W.b3[0] - y0 : 0.0f;
+                e1 = y1 == y1 ? v[1] + S.W.b3[1] - y1 : 0.0f;
             }
             float g0 = 2.0f * e0 * inv_count, g1 = 2.0f * e1 * inv_count;
             float l = warp_sum(e0 * e0 + e1 * e1);
@@ -593,20 +595,27 @@ __global__ void k_adam(float* __restrict__ master, float* __restrict__ grad, flo
 size_t infer_smem_bytes() { return sizeof(InferSmem) + 1024; }
 size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
 
+cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out) {
+    size_t smem = infer_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    uint32_t tiles = (n + kTile - 1) / kTile;
+    uint32_t grid = tiles < (uint32_t)(num_sms * 4) ? tiles : (uint32_t)(num_sms * 4);
+    out->func = (const void*)k_mlp_infer;
+    out->grid = dim3(grid > 0 ? grid : 1);
+    out->block = dim3(kThreads);
+    out->smem = smem;
+    return cudaSuccess;
+}
+
 cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t n,
                   uint32_t* error_flags, cudaStream_t stream, int num_sms) {
     if (n == 0) return cudaSuccess;
-    static bool configured = false;
-    size_t smem = infer_smem_bytes();
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    uint32_t tiles = (n + kTile - 1) / kTile;
-    uint32_t grid = tiles < (uint32_t)(num_sms * 4) ? tiles : (uint32_t)(num_sms * 4);
-    k_mlp_infer<<<grid, kThreads, smem, stream>>>(P, X, out, n, error_flags);
+    KernelLaunch L;
+    cudaError_t e = infer_launch(n, num_sms, &L);
+    if (e != cudaSuccess) return e;
+    k_mlp_infer<<<L.grid, L.block, L.smem, stream>>>(P, X, out, n, error_flags);
     return cudaGetLastError();
 }
 

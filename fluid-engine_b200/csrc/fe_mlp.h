@@ -39,6 +39,16 @@ inline Grads grads_from(float* g, float* loss) {
 }
 
 size_t infer_smem_bytes();
+
+// The inference kernel as a launch description (for CUDA-graph recording):
+// arguments (Params, const __nv_bfloat16* X, float* out, uint32_t n,
+// uint32_t* error_flags).  Sets the kernel's shared-memory attribute.
+struct KernelLaunch {
+    const void* func;
+    dim3 grid, block;
+    size_t smem;
+};
+cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out);
 size_t train_smem_bytes();
 
 // out[i][0..1] for the BF16 rows X[i][0..15], i < n.

@@ -269,6 +269,10 @@ SIGNATURES = {
     "fe_model_train_step": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_float, c_float,
                                     c_void_p, c_void_p]),
     "fe_model_read_flags": (c_int, [c_void_p, POINTER(c_uint32)]),
+    "fe_set_model": (c_int, [CTX, c_void_p]),
+    "fe_capture_begin": (c_int, [CTX, c_uint32, c_uint32]),
+    "fe_capture_read": (c_int, [CTX, c_void_p, c_void_p, c_uint32, POINTER(c_uint32)]),
+    "fe_capture_end": (c_int, [CTX]),
 }
 
 FE_MODEL_PARAMS = 5378

@@ -369,6 +369,22 @@ FE_API fe_status fe_model_train_step(fe_model* model, const float* d_x, const fl
 /* Device error word of the model's kernels (FE_STATS_* bits). */
 FE_API fe_status fe_model_read_flags(fe_model* model, uint32_t* flags);
 
+/* Attaches a model to a context (not owned; NULL detaches).  With
+ * params.warm_start = FE_WARM_LEARNED every substep computes the features
+ * after density_source, runs the network on the tensor cores, starts the
+ * density solve from its first output and the divergence solve from its
+ * second; the Jacobi iterations then run as configured. */
+FE_API fe_status fe_set_model(fe_ctx* ctx, fe_model* model);
+
+/* Training-data capture from the running solver: each substep, one particle
+ * in `stride` (hashed) with a valid Jacobi diagonal records its 12 features
+ * and, after both solves, the two converged pressures in normalised units,
+ * until `capacity` samples are held. */
+FE_API fe_status fe_capture_begin(fe_ctx* ctx, uint32_t capacity, uint32_t stride);
+/* Copies up to `rows` samples: x[rows][12], y[rows][2]; *count = samples held. */
+FE_API fe_status fe_capture_read(fe_ctx* ctx, float* x, float* y, uint32_t rows, uint32_t* count);
+FE_API fe_status fe_capture_end(fe_ctx* ctx);
+
 /* Radix sort that allocates nothing.  No counterpart in the reference: it is
  * for callers that cannot let a library allocate device memory — a frame
  * loop that must not stall (cudaMalloc/cudaFree synchronise the device),

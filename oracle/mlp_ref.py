@@ -71,7 +71,8 @@ def gradients(p, xs, ys, quantize=True):
     w1, w2, w3, b1, b2, b3 = unpack(p)
     n = xs.shape[0]
     out, (X, z1, h1, z2, h2) = forward(p, xs, quantize)
-    e = out - np.asarray(ys, dtype=np.float64)
+    ys = np.asarray(ys, dtype=np.float64)
+    e = np.where(np.isnan(ys), 0.0, out - ys)   # NaN target: output not trained
     g = 2.0 * e / n
     gq = q(g)
     dh2 = gq @ q(w3)

@@ -76,7 +76,6 @@ def test_default_params_match(lib):
     ("dt", float("nan"), _abi.FE_ERR_INVALID_ARGUMENT),
     ("sort_algorithm", 7, _abi.FE_ERR_INVALID_ARGUMENT),
     ("mode", 5, _abi.FE_ERR_INVALID_ARGUMENT),
-    ("warm_start", 1, _abi.FE_ERR_UNSUPPORTED),
 ])
 def test_validate_rejects(lib, field, value, status):
     p = _abi.default_params()
