@@ -438,8 +438,10 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
     const int fixed = c->fixed_mode() ? 1 : 0;
     fe_status s;
     if ((s = rec_simple(c, R, k_viscosity))) return s;
-    if ((s = rec_simple(c, R, k_density_source))) return s;
-    if (c->carries()) REC(R.k(k_features, chunk_grid(c), dim3(kBlock), B, c->L, 0));
+    if (c->carries())
+        REC(R.k(k_density_source_learn, chunk_grid(c), dim3(kBlock), B, c->L));
+    else if ((s = rec_simple(c, R, k_density_source)))
+        return s;
     if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 0));
@@ -449,8 +451,10 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
     if ((s = rec_simple(c, R, k_pressure_integration))) return s;
     if ((s = rec_neighbor_search(c, R))) return s;
     if ((s = rec_simple(c, R, k_density_alpha))) return s;
-    REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));
-    if (c->carries()) REC(R.k(k_features, chunk_grid(c), dim3(kBlock), B, c->L, 1));
+    if (c->carries())
+        REC(R.k(k_divergence_source_learn, chunk_grid(c), dim3(kBlock), B, fixed, c->L));
+    else
+        REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));
     if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 1));

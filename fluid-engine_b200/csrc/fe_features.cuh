@@ -1,0 +1,122 @@
+// fe_features.cuh — the learned warm start's per-particle features, emitted
+// by the two source-term passes (which already visit every neighbour).
+//
+// Normalisation.  With the Jacobi diagonal a_ii = -(dt / rho_i^2) alpha_i, one
+// Jacobi step from zero gives p = -omega s_i rho_i^2 / (dt alpha_i), so
+//   scale_i = rho_i^2 / (dt alpha_i) * (rho0 * 1e-3 / dt)
+// maps a pressure to the units of sigma_i = s_i dt / (rho0 * 1e-3), the
+// source term in 0.1 % density-error units.  The carried pressures enter as
+// kappa / scale_i (0 where alpha_i, rho_i or dt <= 1e-6).  Targets: the
+// density solve's final kappa / scale_i, and the divergence solve's final
+// kappa minus the substep's density kappa (its start without the network),
+// over scale_i.
+//
+// Features (12, standardised with the model's statistics before the network):
+//   0  rho_i / rho0 - 1                    1  alpha_i h^8 / m^2
+//   2  div_i dt / (rho0 1e-3)  (the velocity-divergence term of the source)
+//   3  neighbour count / 32                4  last density kappa / scale_i
+//   5  last divergence kappa / scale_i     6  |v_i| dt / h
+//   7  sigma_i (this solve's source term)
+//   8..11  moments of order 1..4 of the neighbours' density residual,
+//          t_j = x / (1 + |x|) with x = 100 (rho_j / rho0 - 1), weighted by
+//          -grad_factor / (h r) (the list's kernel-gradient scale, >= 0):
+//          sum_j w_j t_j^k / sum_j w_j
+// ("last" = the most recent solve of that kind: before the divergence solve
+// the density kappa is the one just computed in this substep.)
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "fe_common.cuh"
+
+namespace fe {
+
+__device__ __forceinline__ float kappa_scale(float rho, float alpha, float dt, float rho0) {
+    if (!(alpha > kEpsR && rho > kEpsR && dt > kEpsR)) return 0.0f;
+    return (rho * rho / (dt * alpha)) * (rho0 * 1e-3f / dt);
+}
+
+__device__ __forceinline__ float sigma_of(float s, float dt, float rho0) {
+    return s * dt / (rho0 * 1e-3f);
+}
+
+__device__ __forceinline__ uint32_t sample_hash(uint32_t i, uint32_t seed) {
+    uint32_t x = i * 2654435761u ^ (seed * 2246822519u + 0x9E3779B9u);
+    x ^= x >> 15;
+    x *= 2246822519u;
+    x ^= x >> 13;
+    return x;
+}
+
+// Running neighbourhood moments of the density residual.
+struct Moments {
+    float w = 0.0f, m[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    __device__ __forceinline__ void add(float g, float rho_j, float rho0) {
+        float x = 100.0f * (rho_j / rho0 - 1.0f);
+        float t = __fdividef(x, 1.0f + fabsf(x));
+        float wj = -g;
+        w += wj;
+        float p = t;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            m[k] += wj * p;
+            p *= t;
+        }
+    }
+};
+
+// Writes the network input row (learned mode) and captures a sample
+// (capture mode) for particle i before solve `which` (0 density, 1 divergence).
+__device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
+                                              const DevParams& P, uint32_t i, uint32_t scene,
+                                              int which, float src_i, float div_i, f3 v,
+                                              const Moments& mo) {
+    const float h = P.h, m = P.mass, dt = P.dt, rho0 = P.rho0;
+    const float rho = B.rho[i], alpha = B.alpha[i];
+    const float scale = kappa_scale(rho, alpha, dt, rho0);
+    const float4 carry = L.carry[i];
+    float f[12];
+    f[0] = rho / rho0 - 1.0f;
+    const float h2 = h * h, h4 = h2 * h2;
+    f[1] = alpha * (h4 * h4) / (m * m);
+    f[2] = sigma_of(div_i, dt, rho0);
+    const uint32_t cnt = B.nbr_count[i];
+    f[3] = (float)(cnt < 64u ? cnt : 64u) / 32.0f;
+    f[4] = scale > 0.0f ? carry.x / scale : 0.0f;
+    f[5] = scale > 0.0f ? carry.y / scale : 0.0f;
+    f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * dt / h;
+    f[7] = sigma_of(src_i, dt, rho0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) f[8 + k] = mo.w > 0.0f ? mo.m[k] / mo.w : 0.0f;
+
+    if (L.learned) {
+        uint32_t packed[8];
+#pragma unroll
+        for (int k = 0; k < 16; k += 2) {
+            float a = k < 12 ? (f[k] - L.norm[k]) / L.norm[12 + k] : 0.0f;
+            float b = k + 1 < 12 ? (f[k + 1] - L.norm[k + 1]) / L.norm[13 + k] : 0.0f;
+            __nv_bfloat162 two = __floats2bfloat162_rn(a, b);
+            packed[k / 2] = *reinterpret_cast<uint32_t*>(&two);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(L.xb) + (size_t)i * 16);
+        dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+    }
+    uint32_t slot = 0xFFFFFFFFu;
+    if (L.capture && scale > 0.0f &&
+        sample_hash(i, 2u * B.S[scene].substeps + (uint32_t)which) %
+                (L.cap_stride ? L.cap_stride : 1u) == 0u) {
+        uint32_t k = atomicAdd(L.cap_count, 1u);
+        if (k < L.cap_capacity) {
+            slot = k;
+#pragma unroll
+            for (int q = 0; q < 12; ++q) L.cap_x[(size_t)k * 12 + q] = f[q];
+            const float nan = __int_as_float(0x7fffffff);
+            L.cap_y[2 * (size_t)k] = nan;      // the solve fills its own target;
+            L.cap_y[2 * (size_t)k + 1] = nan;  // the other stays NaN (not trained)
+        }
+    }
+    L.carry[i].w = __uint_as_float(slot);
+}
+
+}  // namespace fe

@@ -16,6 +16,7 @@
 // produce identical sums.  A particle with more than kNbrCap neighbours keeps
 // walking the buckets in every pass.
 #include "fe_common.cuh"
+#include "fe_features.cuh"
 #include "fe_kernels.h"
 #include "fe_neighbors.cuh"
 
@@ -198,9 +199,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
 }
 
 // ---------------------------------------------------------------------------
-// density_source_term.comp:16-74 (velocities = velocity_a).
+// density_source_term.comp:16-74 (velocities = velocity_a).  The kLearn
+// variant also emits the warm-start features (same arithmetic for s and p).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
+struct VelRho {
+    float4 v;
+    float rho;
+};
+
+template <bool kLearn>
+__device__ __forceinline__ void density_source_body(const Bufs& B, const LearnArgs& L) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
@@ -208,12 +216,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
     const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(B.vel_a + i));
     float div = 0.0f;
+    Moments mo;
     for_each_neighbor(
-        B, P, i, pi, [&](uint32_t j) { return __ldg(B.vel_a + j); },
-        [&](uint32_t, f3 rv, float g, float4, float4 vj) {
+        B, P, i, pi,
+        [&](uint32_t j) { return VelRho{__ldg(B.vel_a + j), kLearn ? __ldg(B.rho + j) : 0.0f}; },
+        [&](uint32_t, f3 rv, float g, float4, VelRho d) {
             f3 grad = scale(g, rv);
-            f3 vd = sub(vi, xyz(vj));
+            f3 vd = sub(vi, xyz(d.v));
             div += m * dot(vd, grad);
+            if (kLearn) mo.add(g, d.rho, P.rho0);
         });
     float rho_i = B.rho[i];
     float source = 0.0f;
@@ -221,13 +232,23 @@ __global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
     B.src[i] = source;
     B.prs[i] = 0.0f;
     posb(B, i)->w = pressure_over_rho2(0.0f, rho_i);
+    if (kLearn) emit_features(B, L, P, i, s, 0, source, div, vi, mo);
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
+    density_source_body<false>(B, LearnArgs{});
+}
+__global__ void __launch_bounds__(kBlock, 3) k_density_source_learn(Bufs B, LearnArgs L) {
+    density_source_body<true>(B, L);
 }
 
 // ---------------------------------------------------------------------------
 // divergence_source_term.comp:14-61 (velocities = velocity_a in REFERENCE
-// mode, velocity_b in FIXED mode).
+// mode, velocity_b in FIXED mode); kLearn as above.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fixed) {
+template <bool kLearn>
+__device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
+                                                       const LearnArgs& L) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
@@ -236,14 +257,26 @@ __global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fix
     const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(vel + i));
     float div = 0.0f;
+    Moments mo;
     for_each_neighbor(
-        B, P, i, pi, [&](uint32_t j) { return __ldg(vel + j); },
-        [&](uint32_t, f3 rv, float g, float4, float4 vj) {
+        B, P, i, pi,
+        [&](uint32_t j) { return VelRho{__ldg(vel + j), kLearn ? __ldg(B.rho + j) : 0.0f}; },
+        [&](uint32_t, f3 rv, float g, float4, VelRho d) {
             f3 grad = scale(g, rv);
-            f3 vd = sub(vi, xyz(vj));
+            f3 vd = sub(vi, xyz(d.v));
             div += m * dot(vd, grad);
+            if (kLearn) mo.add(g, d.rho, P.rho0);
         });
     B.src[i] = -div;
+    if (kLearn) emit_features(B, L, P, i, s, 1, -div, div, vi, mo);
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fixed) {
+    divergence_source_body<false>(B, fixed, LearnArgs{});
+}
+__global__ void __launch_bounds__(kBlock, 3) k_divergence_source_learn(Bufs B, int fixed,
+                                                                        LearnArgs L) {
+    divergence_source_body<true>(B, fixed, L);
 }
 
 // ---------------------------------------------------------------------------
@@ -277,11 +310,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which)
 // ---------------------------------------------------------------------------
 // pressure_update.comp:18-84, plus the solver control of the tolerance loop.
 // which = 0 (density solve), 1 (divergence solve), -1 (a bare stage call:
-// no control).  The per-particle predicted error of the pressure *before*
-// this update, e_i = max(-(dt * (s_i - Ap_i)), 0) (density) or
-// max(-(s_i - Ap_i), 0) (divergence), is summed in the fixed FP64 order; the
-// last block turns the per-scene sums into the metric, advances the
-// iteration count and sets the loop condition.
+// no control).  The per-particle error of the pressure *before* this update
+// is the projected-Jacobi step in residual units, with r_i = s_i - Ap_i:
+// |r_i| where the update stays positive, p_i |a_ii| / omega where it clamps
+// to 0 (0 for a particle at p = 0 that would go negative, i.e. complementary
+// expansion), and 0 for rows the solver cannot act on (alpha or rho <= 1e-6).
+// It vanishes only at the solution of the clamped system, so an over-
+// estimated pressure counts as error as well as a missing one.  Times dt for
+// the density solve, it is summed in the fixed FP64 order; the last block
+// turns the per-scene sums into the metric, advances the iteration count and
+// sets the loop condition.
 // ---------------------------------------------------------------------------
 __device__ void solve_finish(Bufs& B, int which, cudaGraphConditionalHandle handle,
                              int use_handle, double* smem) {
@@ -348,6 +386,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
         float ap_i = dt * sum_ap;
         float error = s_i - ap_i;
         float p_new = p_i;
+        float e = 0.0f;
         if (alpha_i > kEpsR && rho_i > kEpsR) {
             float a_ii = -(dt / (rho_i * rho_i)) * alpha_i;
             if (fabsf(a_ii) > 1e-20f) {
@@ -355,12 +394,13 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
                 float np = p_i + corr;
                 p_new = np > 0.0f ? np : 0.0f;
                 B.prs[i] = p_new;
+                e = np > 0.0f ? fabsf(error) : (p_i * fabsf(a_ii)) / omega;
             }
         }
         posb(B, i)->w = pressure_over_rho2(p_new, rho_i);
         if (control && P.solver == 1u) {
-            float e = which == 1 ? -error : -(dt * error);
-            e_sum_in = e > 0.0f ? (double)e : 0.0;
+            if (which == 0) e = dt * e;
+            e_sum_in = e > 0.0f ? (double)e : 0.0;  // NaN -> 0
         }
     }
     if (!control) return;

@@ -32,7 +32,8 @@ __global__ void k_divergence_integration(Bufs B, int fixed);
 __global__ void k_stats(Bufs B, int fixed, uint4* upart);
 __global__ void k_frame_prologue(Bufs B);
 __global__ void k_count_substep(Bufs B);
-__global__ void k_features(Bufs B, LearnArgs L, int which);
+__global__ void k_density_source_learn(Bufs B, LearnArgs L);
+__global__ void k_divergence_source_learn(Bufs B, int fixed, LearnArgs L);
 __global__ void k_warm_apply(Bufs B, LearnArgs L, int which);
 __global__ void k_after_solve(Bufs B, LearnArgs L, int which);
 __global__ void k_carry_gather(Bufs B, LearnArgs L);

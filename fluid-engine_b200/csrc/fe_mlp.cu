@@ -126,9 +126,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU with the fast exponential and division intrinsics (the network is
+// BF16; full-precision division would only cost time).
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
-    float s = 1.0f / (1.0f + __expf(-z));
+    float s = __fdividef(1.0f, 1.0f + __expf(-z));
     return s * (1.0f + z * (1.0f - s));
 }
 
@@ -207,97 +209,134 @@ __device__ __forceinline__ void epilogue_silu64(uint32_t taddr, const float* bia
 
 // ---------------------------------------------------------------------------
 // Inference: out[i][0..1] = MLP(x_i) for n rows of X (BF16, 16 per row).
-// 128 TMEM columns: layer-1 and layer-3 accumulators share [0, 64).
+// 256 threads: warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows) and
+// column half w / 4 of each accumulator.  64 TMEM columns are reused by the
+// three layers and one shared buffer holds both hidden activations (each
+// product has finished reading it before the next epilogue overwrites it),
+// so several blocks share an SM.
 // ---------------------------------------------------------------------------
+constexpr int kInferThreads = 256;
+
 struct InferSmem {
     SmemWeights W;
     alignas(128) uint8_t x[kTile * 16 * 2];
-    alignas(128) uint8_t h1[kTile * 64 * 2];
-    alignas(128) uint8_t h2[kTile * 64 * 2];
+    alignas(128) uint8_t h[kTile * 64 * 2];
     alignas(8) uint64_t bar;
     uint32_t tmem_base;
 };
 
-__global__ void __launch_bounds__(kThreads) k_mlp_infer(Params P, const __nv_bfloat16* __restrict__ X,
-                                                        float* __restrict__ out, uint32_t n,
-                                                        uint32_t* error_flags) {
+__device__ __forceinline__ uint32_t lane_addr8(uint32_t base, uint32_t col) {
+    uint32_t warp = threadIdx.x >> 5;
+    return base + (((warp & 3u) * 32u) << 16) + col;
+}
+
+// 32 accumulator columns [c0, c0 + 32) of this warp's rows -> bias + SiLU ->
+// BF16 into the K-major [128 x 64] tile.
+__device__ __forceinline__ void epilogue_half(uint32_t taddr, uint32_t c0, const float* bias,
+                                              uint8_t* out, uint32_t row) {
+#pragma unroll
+    for (uint32_t cc = 0; cc < 32; cc += 16) {
+        float v[16];
+        tmem_ld16(taddr + c0 + cc, v);
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+            __nv_bfloat162 two = __floats2bfloat162_rn(silu(v[i] + bias[c0 + cc + i]),
+                                                       silu(v[i + 1] + bias[c0 + cc + i + 1]));
+            *reinterpret_cast<__nv_bfloat162*>(out + off_k(row, c0 + cc + i, 64)) = two;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
+                                                             const __nv_bfloat16* __restrict__ X,
+                                                             float* __restrict__ out, uint32_t n,
+                                                             uint32_t* error_flags) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
     const uint32_t tid = threadIdx.x;
-    load_weights(S.W, P);
+    const uint32_t warp = tid >> 5, lane = tid & 31u;
+    const uint32_t row = (warp & 3u) * 32u + lane;   // TMEM lane = sample row
+    const uint32_t half = (warp >> 2) * 32u;         // column half
+    for (int t = tid; t < 64 * 16; t += kInferThreads)
+        *reinterpret_cast<__nv_bfloat16*>(S.W.w1 + off_k(t / 16, t % 16, 16)) = P.w1[t];
+    for (int t = tid; t < 64 * 64; t += kInferThreads)
+        *reinterpret_cast<__nv_bfloat16*>(S.W.w2 + off_k(t / 64, t % 64, 64)) = P.w2[t];
+    for (int t = tid; t < 16 * 64; t += kInferThreads) {
+        int o = t / 64, k = t % 64;
+        *reinterpret_cast<__nv_bfloat16*>(S.W.w3 + off_k(o, k, 64)) =
+            o < 2 ? P.w3[o * 64 + k] : __float2bfloat16_rn(0.0f);
+    }
+    if (tid < 64) {
+        S.W.b1[tid] = P.b1[tid];
+        S.W.b2[tid] = P.b2[tid];
+    }
+    if (tid < 16) S.W.b3[tid] = tid < 2 ? P.b3[tid] : 0.0f;
     if (tid == 0) bar_init(&S.bar);
-    tmem_alloc(&S.tmem_base, 128);
+    tmem_alloc(&S.tmem_base, 64);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
-    const uint32_t tbase = S.tmem_base;
-    const uint32_t d1 = tbase, d2 = tbase + 64;
+    const uint32_t d = S.tmem_base;
     uint32_t phase = 0;
     bool ok = true;
     const uint32_t ntiles = (n + kTile - 1) / kTile;
     const uint64_t dx = desc(smem_u32(S.x), 128, 256);
     const uint64_t dw1 = desc(smem_u32(S.W.w1), 128, 256);
     for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const uint32_t row = tid;  // this thread's sample and TMEM lane
-        const uint32_t g = tile * kTile + row;
-        // X tile: one 32-byte row per thread.
+        // X tile: 16 bytes per thread (row tid / 2, half tid % 2).
         {
-            uint4 a = make_uint4(0, 0, 0, 0), b = a;
-            if (g < n) {
-                const uint4* src = reinterpret_cast<const uint4*>(X + (size_t)g * 16);
-                a = src[0];
-                b = src[1];
-            }
-            *reinterpret_cast<uint4*>(S.x + off_k(row, 0, 16)) = a;
-            *reinterpret_cast<uint4*>(S.x + off_k(row, 8, 16)) = b;
+            const uint32_t r = tid >> 1, part = tid & 1u;
+            const uint32_t g = tile * kTile + r;
+            uint4 a = make_uint4(0, 0, 0, 0);
+            if (g < n) a = reinterpret_cast<const uint4*>(X + (size_t)g * 16)[part];
+            *reinterpret_cast<uint4*>(S.x + off_k(r, part * 8, 16)) = a;
         }
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
         if (tid == 0) {
             tc_after_sync();
-            mma(d1, dx, dw1, idesc(128, 64, 0, 0), 0);
+            mma(d, dx, dw1, idesc(128, 64, 0, 0), 0);
             commit(&S.bar);
         }
         ok = __syncthreads_and(bar_wait(&S.bar, phase));
         phase ^= 1;
         tc_after_sync();
-        if (ok) epilogue_silu64(lane_addr(d1, 0), S.W.b1, S.h1, row);
+        if (ok) epilogue_half(lane_addr8(d, 0), half, S.W.b1, S.h, row);
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
         if (tid == 0 && ok) {
             tc_after_sync();
             for (uint32_t kk = 0; kk < 4; ++kk)
-                mma(d2, desc(smem_u32(S.h1) + kk * 256, 128, 1024),
+                mma(d, desc(smem_u32(S.h) + kk * 256, 128, 1024),
                     desc(smem_u32(S.W.w2) + kk * 256, 128, 1024), idesc(128, 64, 0, 0), kk > 0);
             commit(&S.bar);
         }
         ok = __syncthreads_and(ok && bar_wait(&S.bar, phase));
         phase ^= 1;
         tc_after_sync();
-        if (ok) epilogue_silu64(lane_addr(d2, 0), S.W.b2, S.h2, row);
+        if (ok) epilogue_half(lane_addr8(d, 0), half, S.W.b2, S.h, row);
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
         if (tid == 0 && ok) {
             tc_after_sync();
             for (uint32_t kk = 0; kk < 4; ++kk)
-                mma(d1, desc(smem_u32(S.h2) + kk * 256, 128, 1024),
+                mma(d, desc(smem_u32(S.h) + kk * 256, 128, 1024),
                     desc(smem_u32(S.W.w3) + kk * 256, 128, 1024), idesc(128, 16, 0, 0), kk > 0);
             commit(&S.bar);
         }
         ok = __syncthreads_and(ok && bar_wait(&S.bar, phase));
         phase ^= 1;
         tc_after_sync();
-        if (ok) {
+        if (ok && half == 0) {
             float v[16];
-            tmem_ld16(lane_addr(d1, 0), v);
-            if (g < n) {
-                out[2 * (size_t)g] = v[0] + S.W.b3[0];
-                out[2 * (size_t)g + 1] = v[1] + S.W.b3[1];
-            }
+            tmem_ld16(lane_addr8(d, 0), v);
+            const uint32_t g = tile * kTile + row;
+            if (g < n)
+                reinterpret_cast<float2*>(out)[g] = make_float2(v[0] + S.W.b3[0], v[1] + S.W.b3[1]);
         }
         tc_before_sync();
         __syncthreads();
@@ -307,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) k_mlp_infer(Params P, const __nv_bfl
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
-    tmem_free(tbase, 128);
+    tmem_free(d, 64);
 }
 
 // ---------------------------------------------------------------------------
@@ -601,10 +640,10 @@ cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out) {
                                          (int)smem);
     if (e != cudaSuccess) return e;
     uint32_t tiles = (n + kTile - 1) / kTile;
-    uint32_t grid = tiles < (uint32_t)(num_sms * 4) ? tiles : (uint32_t)(num_sms * 4);
+    uint32_t grid = tiles < (uint32_t)(num_sms * 6) ? tiles : (uint32_t)(num_sms * 6);
     out->func = (const void*)k_mlp_infer;
     out->grid = dim3(grid > 0 ? grid : 1);
-    out->block = dim3(kThreads);
+    out->block = dim3(kInferThreads);
     out->smem = smem;
     return cudaSuccess;
 }

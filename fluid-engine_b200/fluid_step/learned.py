@@ -2,7 +2,8 @@
 
 The network (12 -> 64 -> 64 -> 2, SiLU, BF16 tensor cores; see fe_mlp.cu)
 predicts the initial pressure of the density and divergence solves from 12
-per-particle features (fe_learned.cu).  It is trained on pairs that the plain
+per-particle features (fe_features.cuh), which the two source-term passes
+emit as they walk each particle's neighbours.  It is trained on pairs that the plain
 Jacobi solver produces: with capture on, each substep records a hashed sample
 of particles' features and, after both solves, their converged pressures in
 normalised units.  Training runs on the GPU with the library's own forward,
@@ -86,9 +87,14 @@ class TrainResult:
     samples: int
 
 
-def capture(workload_names=("dam_break_16k", "dam_break_256k"), frames=(60, 12),
-            strides=(4, 24), capacity=120_000, warmup=2, device=0, seed=1):
-    """Runs the plain tolerance solver and returns captured (x[n][12], y[n][2])."""
+def capture(workload_names=("dam_break_16k", "dam_break_256k"), frames=(100, 300),
+            strides=(32, 1536), capacity=120_000, warmup=2, device=0, seed=1):
+    """Runs the plain tolerance solver and returns captured (x[n][12], y[n][2]).
+
+    The defaults sample the 16,384-particle dam break (fixed dt 1 ms) over 100
+    frames and the 262,144-particle one (adaptive CFL) over 300 frames, about
+    100k solve snapshots each: a sample is taken for a (particle, substep,
+    solve) triple whose hash is 0 modulo the stride."""
     lib = load_library()
     xs, ys = [], []
     for name, nf, stride in zip(workload_names, frames, strides):
@@ -187,8 +193,8 @@ def evaluate(model: Model, x: np.ndarray, y: np.ndarray) -> float:
 def compare_iterations(model: Model, workload: str = "dam_break_16k", frames: int = 20,
                        warmup: int = 5, min_iterations: int = 1, device: int = 0):
     """Plain versus learned warm start on the same scene and tolerance:
-    average Jacobi iterations per frame (density, divergence) and the final
-    residual metrics."""
+    average Jacobi iterations per frame (density, divergence), the largest
+    residual metrics and speed seen, and the simulated time covered."""
     lib = load_library()
     out = {}
     for arm in ("plain", "learned"):
@@ -206,9 +212,11 @@ def compare_iterations(model: Model, workload: str = "dam_break_16k", frames: in
             sim.step(1)
         st0 = sim.data.read_stats()
         res = []
+        sim_time = 0.0
         for _ in range(frames):
             st = sim.step(1)
-            res.append((st.density_residual, st.divergence_residual))
+            res.append((st.density_residual, st.divergence_residual, st.max_speed))
+            sim_time += st.dt
         st = sim.data.read_stats()
         out[arm] = {
             "density_iterations": (st.total_density_iterations - st0.total_density_iterations) / frames,
@@ -216,7 +224,10 @@ def compare_iterations(model: Model, workload: str = "dam_break_16k", frames: in
                                       - st0.total_divergence_iterations) / frames,
             "max_density_residual": float(max(r[0] for r in res)),
             "max_divergence_residual": float(max(r[1] for r in res)),
+            "max_speed": float(max(r[2] for r in res)),
+            "simulated_seconds": sim_time,
             "cap_hits": int(st.flags & _abi.FE_STATS_ITERATION_CAP_HIT),
+            "non_finite": int(st.flags & _abi.FE_STATS_NON_FINITE),
         }
         sim.close()
     return out

@@ -14,6 +14,7 @@ Dam-break workloads (particle-steps/s benchmarks and parity cases):
                   rho0 1000, m 0.125, h 0.1, nu 0.01, dt 1 ms, K 4+4, radix
   dam_break_256k  64^3 lattice in [0,4]^3, adaptive CFL, tolerance 0.1 %
   dam_break_1m    128x64x128 lattice in [0,8]x[0,4]x[0,8], tolerance 0.1 %
+  dam_break_1m_cfl  the same scene with the adaptive CFL step of the 262k one
   dam_break_4m    256x64x256 lattice in [0,16]x[0,4]x[0,16] (the 1M scene
                   widened in x and z at the same fill), tolerance 0.1 %
 All start at rest; the lattice origin is box_min, shifted by the particle
@@ -109,6 +110,7 @@ def dam_break_params(box_min, box_max, *, solver=_abi.FE_SOLVER_FIXED_ITERS,
     p.solver = solver
     p.density_tolerance = 0.001
     p.divergence_tolerance = 0.001
+    p.min_iterations = 1
     return p
 
 
@@ -124,6 +126,11 @@ def workload(name: str) -> Workload:
     elif name == "dam_break_1m":
         w = Workload(name, (128, 64, 128), (0.0, 0.0, 0.0), (8.0, 4.0, 8.0), 200)
         w.params = dam_break_params(w.box_min, w.box_max,
+                                    solver=_abi.FE_SOLVER_TOLERANCE,
+                                    mode=_abi.FE_MODE_FIXED)
+    elif name == "dam_break_1m_cfl":
+        w = Workload(name, (128, 64, 128), (0.0, 0.0, 0.0), (8.0, 4.0, 8.0), 200)
+        w.params = dam_break_params(w.box_min, w.box_max, use_cfl=True,
                                     solver=_abi.FE_SOLVER_TOLERANCE,
                                     mode=_abi.FE_MODE_FIXED)
     elif name == "dam_break_1m_k4":

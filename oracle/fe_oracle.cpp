@@ -564,10 +564,11 @@ struct State : Base {
     }
 
     // pressure_update.comp:18-84.  With want_residual, also returns the
-    // fixed-order FP64 sum of the per-particle predicted error of the
-    // pressure *before* this update (tolerance solver, no reference
-    // counterpart): density solve e_i = max(-(dt * (s_i - Ap_i)), 0),
-    // divergence solve e_i = max(-(s_i - Ap_i), 0).
+    // fixed-order FP64 sum of the per-particle error of the pressure *before*
+    // this update (tolerance solver, no reference counterpart): the
+    // projected-Jacobi step in residual units, r_i = s_i - Ap_i, is |r_i|
+    // where the update stays positive, p_i |a_ii| / omega where it clamps to
+    // 0, and 0 for rows the update skips; times dt for the density solve.
     std::vector<double> resid;
     double pressure_update(bool want_residual, bool divergence) override {
         R m = mass(), hh = h(), d = dt(), omega = (R)p.relax_factor, eps = K<R>::eps_r();
@@ -588,16 +589,18 @@ struct State : Base {
             });
             R ap_i = d * sum_ap;
             R error = s_i - ap_i;
+            R e = 0;
             if (alpha_i > eps && rho_i > eps) {
                 R a_ii = -(d / (rho_i * rho_i)) * alpha_i;
                 if (std::fabs(a_ii) > R(1e-20)) {
                     R corr = (omega * error) / a_ii;
                     R np = p_i + corr;
                     prs[i] = np > R(0) ? np : R(0);  // max(x, 0.0), NaN -> 0
+                    e = np > R(0) ? std::fabs(error) : (p_i * std::fabs(a_ii)) / omega;
                 }
             }
             if (want_residual) {
-                R e = divergence ? -error : -(d * error);
+                if (!divergence) e = d * e;
                 resid[i] = e > R(0) ? (double)e : 0.0;
             }
         }
@@ -807,9 +810,8 @@ void frame_prologue(Base* s) {
     s->iters_div = (early && avg_ve < thr_v) ? 1u : p.divergence_solver_iterations;
 }
 
-// The tolerance metric from the residual sum: mean predicted density error
-// over ρ0 (density solve) and mean predicted dρ/dt · dt over ρ0 (divergence
-// solve).  The device computes the same expression in double.
+// The tolerance metric from the residual sum: mean density error over ρ0
+// (density solve) and mean dρ/dt · dt over ρ0 (divergence solve).  The device computes the same expression in double.
 double solver_metric(Base* s, double sum, bool divergence) {
     double avg = sum / (double)s->n;
     if (divergence) avg = avg * (double)s->p.dt;
