@@ -374,6 +374,77 @@ def full_run(w, params, model, local, frames=None):
     return out
 
 
+def run_batch(args, world, rank, local):
+    """The 64 batched dam-break scenes: this rank's LPT share of the scenes in
+    one batch context (no collective inside a step), W warm-up frames, then K
+    frames timed with CUDA events on the context stream; the time is the max
+    over ranks and the value counts every scene's particles (strong scaling:
+    the 64 scenes are fixed).  At N=1 the same scenes also run as 64 separate
+    contexts stepped one after another, for comparison.  Per-scene stats are
+    all-gathered after the timed region."""
+    import torch
+
+    from fluid_step import scene
+    from fluid_step.pipelines import BatchSimulation, Simulation
+    from fluid_step.sharding import gather_scene_stats, imbalance, lpt_partition, stats_row
+
+    w = scene.batch_workload()
+    parts = lpt_partition(w.counts, world)
+    mine = parts[rank]
+    pos, par = w.positions(), w.params()
+    total = int(sum(w.counts))
+    sim = BatchSimulation([pos[k] for k in mine], [par[k] for k in mine], device=local)
+    lib, h = sim.data._lib, sim.data.handle
+    stream = torch.cuda.ExternalStream(lib.fe_get_stream(h), device=local)
+    for _ in range(args.warmup):
+        sim.step(1)
+    barrier(world)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        a.record(stream)
+        for _ in range(args.steps):
+            rc = lib.fe_step(h, 1, 0, None)
+            if rc:
+                raise RuntimeError(f"fe_step (batch) failed: {rc}")
+        b.record(stream)
+        b.synchronize()
+    ms = reduce_max(a.elapsed_time(b), world)
+    rows = [stats_row(sim.data.read_scene_stats(i)) for i in range(len(mine))]
+    sim.close()
+    table = gather_scene_stats(mine, rows, len(w.counts),
+                               device=f"cuda:{local}" if world > 1 else None)
+    out = {"workload": w.name, "scenes": len(w.counts), "particles": total,
+           "counts_min_max": [min(w.counts), max(w.counts)],
+           "value": total * args.steps / (ms / 1e3), "unit": "particle-steps/s",
+           "ms_per_step": ms / args.steps, "scaling": "strong", "ranks": world,
+           "partition_imbalance": imbalance(w.counts, parts),
+           "physics": "dt 1 ms, 4 + 4 Jacobi iterations, REFERENCE mode, radix sort, "
+                      "per-scene XSPH coefficient",
+           "non_finite_scenes": int(np.sum(table[:, -1].astype(np.int64) & 0x8 != 0)),
+           "clocks": clocks.summary()}
+    if world == 1:
+        sims = [Simulation(pos[k], par[k], device=local) for k in range(len(w.counts))]
+        for _ in range(args.warmup):
+            for s_ in sims:
+                s_.step(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for s_ in sims:
+                s_.data._lib.fe_step(s_.data.handle, 1, 0, None)
+        for s_ in sims:
+            s_.data._lib.fe_synchronize(s_.data.handle)
+        seq = time.perf_counter() - t0
+        for s_ in sims:
+            s_.close()
+        out["separate_contexts"] = {"value": total * args.steps / seq,
+                                    "ms_per_step": seq * 1e3 / args.steps,
+                                    "timing": "host clock: 64 contexts, one fe_step each per "
+                                              "frame, one stream each"}
+    return out
+
+
 def run_gpu(args) -> None:
     import torch
 
@@ -424,6 +495,7 @@ def run_gpu(args) -> None:
             if "learned" in r and "plain" in r and r["plain"]["ms_per_step"]:
                 r["learned_over_plain"] = r["plain"]["ms_per_step"] / r["learned"]["ms_per_step"]
             runs[name] = r
+    batch = run_batch(args, world, rank, local) if args.batch else None
     head = arms["learned"] if "learned" in arms else arms["plain"]
     lib = _abi.load_library()
     sort = sort_benchmark(lib)
@@ -491,6 +563,8 @@ def run_gpu(args) -> None:
         }
         if runs:
             out["full_runs"] = runs
+        if batch:
+            out["batched"] = batch
         if "learned" in arms and "plain" in arms:
             pl = arms["plain"]
             out["plain_jacobi"] = {"value": pl["value"], "ms_per_step": pl["dev_ms"] / args.steps,
@@ -617,6 +691,8 @@ def main():
                     help="eager frames, then one launch of each hot pass (for ncu -k)")
     ap.add_argument("--eager", action="store_true",
                     help="launch frames without CUDA graphs (for profilers)")
+    ap.add_argument("--no-batch", dest="batch", action="store_false",
+                    help="skip the 64-scene batched dam break")
     ap.add_argument("--no-full-runs", dest="full_runs", action="store_false",
                     help="skip the whole runs (1M dam break 200 steps, 262k adaptive-CFL "
                          "dam break 1000 steps) of both arms")

@@ -462,13 +462,13 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
     if ((s = rec_solve(c, R, 1))) return s;
     if (c->carries()) REC(R.k(k_after_solve, chunk_grid(c), dim3(kBlock), B, c->L, 1));
     REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), B, fixed));
-    REC(R.k(k_count_substep, dim3(1), dim3(64), B));
+    REC(R.k(k_count_substep, dim3((B.n_scenes + 63) / 64), dim3(64), B));
     return FE_OK;
 }
 
 fe_status rec_frame(fe_ctx* c, Recorder& R, uint32_t n_substeps, bool init) {
     fe_status s;
-    REC(R.k(k_frame_prologue, dim3(1), dim3(64), c->B));
+    REC(R.k(k_frame_prologue, dim3((c->B.n_scenes + 63) / 64), dim3(64), c->B));
     if (init) {
         if ((s = rec_neighbor_search(c, R))) return s;
         if ((s = rec_simple(c, R, k_density_alpha))) return s;
@@ -579,15 +579,15 @@ fe_status get_graph(fe_ctx* c, uint32_t n_substeps, bool init, cudaGraphExec_t* 
     return FE_OK;
 }
 
-fe_status collect_stats(fe_ctx* c, fe_stats* out) {
-    FE_CUDA(cudaMemcpyAsync(c->h_state, c->B.S, sizeof(SceneState), cudaMemcpyDeviceToHost,
-                            c->stream));
+fe_status collect_stats(fe_ctx* c, fe_stats* out, uint32_t scene = 0) {
+    FE_CUDA(cudaMemcpyAsync(c->h_state + scene, c->B.S + scene, sizeof(SceneState),
+                            cudaMemcpyDeviceToHost, c->stream));
     FE_CUDA(cudaMemcpyAsync(c->h_global, c->B.G, sizeof(GlobalState), cudaMemcpyDeviceToHost,
                             c->stream));
     DevParams dp;
-    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P + scene, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
     FE_CUDA(cudaStreamSynchronize(c->stream));
-    const SceneState& S = *c->h_state;
+    const SceneState& S = c->h_state[scene];
     std::memset(out, 0, sizeof *out);
     out->max_speed_bits = S.stats[0];
     out->density_error_fp = S.stats[1];
@@ -606,11 +606,11 @@ fe_status collect_stats(fe_ctx* c, fe_stats* out) {
     out->total_density_iterations = S.total_iters[0];
     out->total_divergence_iterations = S.total_iters[1];
     out->substeps = S.substeps;
-    uint32_t flags = c->h_global->flags;
+    uint32_t flags = c->h_global->flags;  // cap hit and look-back timeout: any scene
     if (S.nonfinite) flags |= 0x8u;
     out->flags = flags;
     // host-side mirror of the device dt
-    c->params[0].dt = dp.dt;
+    c->params[scene].dt = dp.dt;
     return FE_OK;
 }
 
@@ -689,19 +689,63 @@ void fe_default_params(fe_params* p) {
 
 fe_status fe_validate_params(const fe_params* p) { return validate(p); }
 
-fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
-                    const float* vel_xyz, int device, fe_ctx** out) {
+namespace {
+
+// The scenes of one context must share what is recorded once per frame for
+// all of them: the sort (bitonic is single-scene), the buffer pairing mode
+// and the warm start.  Everything else (physics, time step, solver and its
+// tolerance) is per scene.
+fe_status check_batch_uniform(const fe_params& a, const fe_params& b, uint32_t n_scenes) {
+    if (n_scenes > 1 && (a.sort_algorithm != FE_SORT_RADIX || b.sort_algorithm != FE_SORT_RADIX)) {
+        set_error("bitonic sort is single-scene only");
+        return FE_ERR_UNSUPPORTED;
+    }
+    if (a.mode != b.mode || a.warm_start != b.warm_start || a.sort_algorithm != b.sort_algorithm) {
+        set_error("scenes of one context must share mode, warm_start and sort_algorithm");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    return FE_OK;
+}
+
+// A context over n_scenes independent scenes laid out back to back: scene s
+// owns particles [first_s, first_s + n_s), hash-table slots
+// [base_s, base_s + T_s) with T_s = next_pow2(n_s), and ceil(n_s / 256)
+// chunks of the chunk table.  Keys are base_s + hash_s, so one stable sort
+// of all keys orders every scene by (hash, index) within its own range, and
+// each scene's chunks, reductions and solver control are those it has alone.
+fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n_scenes,
+                     const float* pos_xyz, const float* vel_xyz, int device, fe_ctx** out) {
     if (!out) {
         set_error("out is NULL");
         return FE_ERR_INVALID_ARGUMENT;
     }
     *out = nullptr;
-    fe_status s = validate(params);
-    if (s != FE_OK) return s;
-    if (n == 0 || n > FE_MAX_PARTICLES) {
-        set_error("particle count %u outside 1..%u", n, FE_MAX_PARTICLES);
-        return n == 0 ? FE_ERR_INVALID_ARGUMENT : FE_ERR_CAPACITY;
+    if (!params || !counts || n_scenes == 0) {
+        set_error("params and counts must be given for at least one scene");
+        return FE_ERR_INVALID_ARGUMENT;
     }
+    if (n_scenes > FE_MAX_SCENES) {
+        set_error("%u scenes above FE_MAX_SCENES (%u)", n_scenes, FE_MAX_SCENES);
+        return FE_ERR_CAPACITY;
+    }
+    fe_status s;
+    uint64_t n64 = 0, t64 = 0;
+    for (uint32_t k = 0; k < n_scenes; ++k) {
+        if ((s = validate(&params[k])) != FE_OK) return s;
+        if ((s = check_batch_uniform(params[0], params[k], n_scenes)) != FE_OK) return s;
+        if (counts[k] == 0 || counts[k] > FE_MAX_PARTICLES) {
+            set_error("scene %u: particle count %u outside 1..%u", k, counts[k], FE_MAX_PARTICLES);
+            return counts[k] == 0 ? FE_ERR_INVALID_ARGUMENT : FE_ERR_CAPACITY;
+        }
+        n64 += counts[k];
+        t64 += next_pow2(counts[k]);
+    }
+    if (n64 > FE_MAX_PARTICLES || t64 > (1ull << 31)) {
+        set_error("%llu particles (%llu table slots) above FE_MAX_PARTICLES",
+                  (unsigned long long)n64, (unsigned long long)t64);
+        return FE_ERR_CAPACITY;
+    }
+    const uint32_t n = (uint32_t)n64;
     if (!pos_xyz) {
         set_error("pos_xyz is NULL");
         return FE_ERR_INVALID_ARGUMENT;
@@ -725,11 +769,23 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
     fe_ctx* c = new fe_ctx();
     c->device = device;
     c->n = n;
-    c->T = next_pow2(n);
+    c->T = (uint32_t)t64;
     c->key_bits = log2_ceil(c->T);
     if (c->key_bits == 0) c->key_bits = 1;
-    c->params.assign(1, *params);
-    c->dparams.assign(1, to_device(*params, n, c->T, 0, 0));
+    c->params.assign(params, params + n_scenes);
+    std::vector<uint4> hc;
+    {
+        uint32_t first = 0, base = 0;
+        for (uint32_t k = 0; k < n_scenes; ++k) {
+            const uint32_t nk = counts[k], tk = next_pow2(nk);
+            c->dparams.push_back(to_device(params[k], nk, tk, base, first));
+            for (uint32_t q = 0; q * kBlock < nk; ++q)
+                hc.push_back(make_uint4(first + q * kBlock, std::min<uint32_t>(kBlock, nk - q * kBlock),
+                                        k, (uint32_t)hc.size()));
+            first += nk;
+            base += tk;
+        }
+    }
     auto fail = [&](fe_status st) {
         release(c);
         delete c;
@@ -741,11 +797,11 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
     }
     Bufs& B = c->B;
     std::memset(&B, 0, sizeof B);
-    const uint32_t nchunks = (n + kBlock - 1) / kBlock;
+    const uint32_t nchunks = (uint32_t)hc.size();
     B.n_total = n;
     B.T_total = c->T;
     B.n_chunks = nchunks;
-    B.n_scenes = 1;
+    B.n_scenes = n_scenes;
     uint4* chunks_d = nullptr;
     const size_t scratch_words = radix_scratch_words(n, c->key_bits);
     if ((s = dev_alloc(c, &B.pos_a, n)) || (s = dev_alloc(c, &B.pos_b, n)) ||
@@ -757,15 +813,15 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
         (s = dev_alloc(c, &B.keys, c->T)) ||
         (s = dev_alloc(c, &B.vals, c->T)) || (s = dev_alloc(c, &B.cells, c->T)) ||
         (s = dev_alloc(c, &B.nbr_count, n)) || (s = dev_alloc(c, &B.nbr, (size_t)kNbrCap * n)) ||
-        (s = dev_alloc(c, &chunks_d, nchunks)) || (s = dev_alloc(c, &B.P, 1)) ||
-        (s = dev_alloc(c, &B.S, 1)) || (s = dev_alloc(c, &B.G, 1)) ||
+        (s = dev_alloc(c, &chunks_d, nchunks)) || (s = dev_alloc(c, &B.P, n_scenes)) ||
+        (s = dev_alloc(c, &B.S, n_scenes)) || (s = dev_alloc(c, &B.G, 1)) ||
         (s = dev_alloc(c, &B.partials, 2 * (size_t)nchunks)) ||
         (s = dev_alloc(c, &c->upart, nchunks)) || (s = dev_alloc(c, &c->tmp_keys, n)) ||
         (s = dev_alloc(c, &c->tmp_vals, n)) ||
         (s = dev_alloc(c, &c->sort_scratch, scratch_words)))
         return fail(s);
     B.chunks = chunks_d;
-    if (cudaMallocHost(&c->h_state, sizeof(SceneState)) != cudaSuccess ||
+    if (cudaMallocHost(&c->h_state, sizeof(SceneState) * n_scenes) != cudaSuccess ||
         cudaMallocHost(&c->h_global, sizeof(GlobalState)) != cudaSuccess) {
         set_error("cudaMallocHost failed");
         return fail(FE_ERR_OUT_OF_MEMORY);
@@ -774,9 +830,6 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
     std::vector<float4> h4(n);
     for (uint32_t i = 0; i < n; ++i)
         h4[i] = make_float4(pos_xyz[3 * i], pos_xyz[3 * i + 1], pos_xyz[3 * i + 2], 1.0f);
-    std::vector<uint4> hc(nchunks);
-    for (uint32_t k = 0; k < nchunks; ++k)
-        hc[k] = make_uint4(k * kBlock, std::min<uint32_t>(kBlock, n - k * kBlock), 0, k);
     auto setup = [&]() -> fe_status {
         FE_CUDA(cudaMemcpy(B.pos_a, h4.data(), (size_t)n * 16, cudaMemcpyHostToDevice));
         for (uint32_t i = 0; i < n; ++i)
@@ -797,9 +850,10 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
             FE_CUDA(cudaMemset(B.vals + n, 0xFF, (size_t)(c->T - n) * 4));
         }
         FE_CUDA(cudaMemset(B.cells, 0xFF, (size_t)c->T * 8));
-        FE_CUDA(cudaMemset(B.S, 0, sizeof(SceneState)));
+        FE_CUDA(cudaMemset(B.S, 0, sizeof(SceneState) * n_scenes));
         FE_CUDA(cudaMemset(B.G, 0, sizeof(GlobalState)));
-        FE_CUDA(cudaMemcpy(B.P, c->dparams.data(), sizeof(DevParams), cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemcpy(B.P, c->dparams.data(), sizeof(DevParams) * n_scenes,
+                           cudaMemcpyHostToDevice));
         fe_status st = run_refresh_pr(c);
         if (st != FE_OK) return st;
         FE_CUDA(cudaStreamSynchronize(c->stream));
@@ -810,6 +864,48 @@ fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
     return FE_OK;
 }
 
+}  // namespace
+
+fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
+                    const float* vel_xyz, int device, fe_ctx** out) {
+    if (n == 0 || n > FE_MAX_PARTICLES) {
+        if (out) *out = nullptr;
+        set_error("particle count %u outside 1..%u", n, FE_MAX_PARTICLES);
+        return n == 0 ? FE_ERR_INVALID_ARGUMENT : FE_ERR_CAPACITY;
+    }
+    return create_ctx(params, &n, 1, pos_xyz, vel_xyz, device, out);
+}
+
+fe_status fe_batch_create(const fe_params* params, const uint32_t* counts, uint32_t n_scenes,
+                          const float* pos_xyz, const float* vel_xyz, int device, fe_ctx** out) {
+    return create_ctx(params, counts, n_scenes, pos_xyz, vel_xyz, device, out);
+}
+
+fe_status fe_scene_count(const fe_ctx* c, uint32_t* out) {
+    if (!c || !out) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    *out = c->B.n_scenes;
+    return FE_OK;
+}
+
+fe_status fe_scene_table(const fe_ctx* c, uint32_t* first, uint32_t* count, uint32_t capacity) {
+    if (!c || !first || !count) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (capacity < c->B.n_scenes) {
+        set_error("capacity %u below the %u scenes", capacity, c->B.n_scenes);
+        return FE_ERR_CAPACITY;
+    }
+    for (uint32_t k = 0; k < c->B.n_scenes; ++k) {
+        first[k] = c->dparams[k].first;
+        count[k] = c->dparams[k].n;
+    }
+    return FE_OK;
+}
+
 fe_status fe_destroy(fe_ctx* c) {
     if (!c) return FE_OK;
     release(c);
@@ -817,22 +913,61 @@ fe_status fe_destroy(fe_ctx* c) {
     return FE_OK;
 }
 
-fe_status fe_set_params(fe_ctx* c, const fe_params* p) {
-    if (!c) {
-        set_error("context is NULL");
-        return FE_ERR_INVALID_ARGUMENT;
-    }
+namespace {
+
+fe_status set_scene_params(fe_ctx* c, uint32_t first, uint32_t last, const fe_params* p) {
     fe_status s = validate(p);
     if (s != FE_OK) return s;
-    if (p->sort_algorithm == FE_SORT_BITONIC && c->B.n_scenes > 1) {
+    const uint32_t ns = c->B.n_scenes;
+    // Every scene must keep sharing what one frame records for all of them.
+    for (uint32_t k = 0; k < ns; ++k) {
+        if (k >= first && k < last) continue;
+        if ((s = check_batch_uniform(c->params[k], *p, ns)) != FE_OK) return s;
+    }
+    if (ns > 1 && p->sort_algorithm != FE_SORT_RADIX) {
         set_error("bitonic sort is single-scene only");
         return FE_ERR_UNSUPPORTED;
     }
     FE_CUDA(cudaSetDevice(c->device));
-    c->params[0] = *p;
-    const DevParams& old = c->dparams[0];
-    c->dparams[0] = to_device(*p, old.n, old.T, old.table_base, old.first);
+    for (uint32_t k = first; k < last; ++k) {
+        c->params[k] = *p;
+        const DevParams& old = c->dparams[k];
+        c->dparams[k] = to_device(*p, old.n, old.T, old.table_base, old.first);
+    }
     return upload_params(c);
+}
+
+fe_status get_scene_params(const fe_ctx* c, uint32_t scene, fe_params* out) {
+    fe_ctx* m = const_cast<fe_ctx*>(c);
+    FE_CUDA(cudaSetDevice(c->device));
+    DevParams dp;
+    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P + scene, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    m->params[scene].dt = dp.dt;
+    *out = c->params[scene];
+    return FE_OK;
+}
+
+}  // namespace
+
+fe_status fe_set_params(fe_ctx* c, const fe_params* p) {
+    if (!c || !p) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    return set_scene_params(c, 0, c->B.n_scenes, p);
+}
+
+fe_status fe_set_scene_params(fe_ctx* c, uint32_t scene, const fe_params* p) {
+    if (!c || !p) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (scene >= c->B.n_scenes) {
+        set_error("scene %u of %u", scene, c->B.n_scenes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    return set_scene_params(c, scene, scene + 1, p);
 }
 
 fe_status fe_get_params(const fe_ctx* c, fe_params* out) {
@@ -840,14 +975,19 @@ fe_status fe_get_params(const fe_ctx* c, fe_params* out) {
         set_error("NULL argument");
         return FE_ERR_INVALID_ARGUMENT;
     }
-    fe_ctx* m = const_cast<fe_ctx*>(c);
-    FE_CUDA(cudaSetDevice(c->device));
-    DevParams dp;
-    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
-    FE_CUDA(cudaStreamSynchronize(c->stream));
-    m->params[0].dt = dp.dt;
-    *out = c->params[0];
-    return FE_OK;
+    return get_scene_params(c, 0, out);
+}
+
+fe_status fe_get_scene_params(const fe_ctx* c, uint32_t scene, fe_params* out) {
+    if (!c || !out) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (scene >= c->B.n_scenes) {
+        set_error("scene %u of %u", scene, c->B.n_scenes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    return get_scene_params(c, scene, out);
 }
 
 fe_status fe_prepare(fe_ctx* c) {
@@ -966,6 +1106,19 @@ fe_status fe_read_stats(fe_ctx* c, fe_stats* out) {
     }
     FE_CUDA(cudaSetDevice(c->device));
     return collect_stats(c, out);
+}
+
+fe_status fe_read_scene_stats(fe_ctx* c, uint32_t scene, fe_stats* out) {
+    if (!c || !out) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (scene >= c->B.n_scenes) {
+        set_error("scene %u of %u", scene, c->B.n_scenes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    return collect_stats(c, out, scene);
 }
 
 fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {

@@ -77,6 +77,7 @@ FE_STATS_LOOKBACK_TIMEOUT = 0x4
 FE_STATS_NON_FINITE = 0x8
 
 FE_MAX_PARTICLES = 1 << 26
+FE_MAX_SCENES = 65536
 
 
 class FeParams(Structure):
@@ -235,6 +236,13 @@ SIGNATURES = {
     "fe_create": (c_int, [POINTER(FeParams), c_uint32, c_void_p, c_void_p, c_int,
                           POINTER(CTX)]),
     "fe_destroy": (c_int, [CTX]),
+    "fe_batch_create": (c_int, [POINTER(FeParams), POINTER(c_uint32), c_uint32, c_void_p,
+                                c_void_p, c_int, POINTER(CTX)]),
+    "fe_scene_count": (c_int, [CTX, POINTER(c_uint32)]),
+    "fe_scene_table": (c_int, [CTX, POINTER(c_uint32), POINTER(c_uint32), c_uint32]),
+    "fe_set_scene_params": (c_int, [CTX, c_uint32, POINTER(FeParams)]),
+    "fe_get_scene_params": (c_int, [CTX, c_uint32, POINTER(FeParams)]),
+    "fe_read_scene_stats": (c_int, [CTX, c_uint32, POINTER(FeStats)]),
     "fe_set_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_get_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_prepare": (c_int, [CTX]),

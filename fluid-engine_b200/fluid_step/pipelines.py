@@ -238,6 +238,78 @@ class Simulation:
         self.data.close()
 
 
+class BatchPhysicsData(GpuPhysicsData):
+    """Many independent scenes in one context (fe_batch_create): the
+    per-scene GpuPhysicsData of the reference, laid out back to back.
+    Fields download and upload as one array over all scenes; `scene(a, s)`
+    is scene s's slice of such an array."""
+
+    def __init__(self, scene_positions, scene_params, *, scene_velocities=None, device: int = 0):
+        self._lib = load_library()
+        pos = [np.ascontiguousarray(p, dtype=np.float32).reshape(-1, 3) for p in scene_positions]
+        if len(pos) != len(scene_params) or not pos:
+            raise ValueError("one parameter block per scene, at least one scene")
+        counts = (ctypes.c_uint32 * len(pos))(*[p.shape[0] for p in pos])
+        params = (_abi.FeParams * len(pos))(*[_abi.copy_params(q) for q in scene_params])
+        allpos = np.ascontiguousarray(np.concatenate(pos))
+        vel = None
+        if scene_velocities is not None:
+            vel = np.ascontiguousarray(np.concatenate(
+                [np.asarray(v, dtype=np.float32).reshape(-1, 3) for v in scene_velocities]))
+        self.count = int(allpos.shape[0])
+        self.params = _abi.copy_params(scene_params[0])
+        h = ctypes.c_void_p()
+        st = self._lib.fe_batch_create(params, counts, len(pos),
+                                       allpos.ctypes.data_as(ctypes.c_void_p),
+                                       None if vel is None else vel.ctypes.data_as(ctypes.c_void_p),
+                                       device, ctypes.byref(h))
+        check(self._lib, st, "fe_batch_create")
+        self.handle = h
+        n, t = ctypes.c_uint32(), ctypes.c_uint32()
+        check(self._lib, self._lib.fe_get_size(h, ctypes.byref(n), ctypes.byref(t)), "fe_get_size")
+        self.table_size = int(t.value)
+        ns = len(pos)
+        first, cnt = (ctypes.c_uint32 * ns)(), (ctypes.c_uint32 * ns)()
+        check(self._lib, self._lib.fe_scene_table(h, first, cnt, ns), "fe_scene_table")
+        self.scene_first = np.array(first[:], dtype=np.int64)
+        self.scene_count = np.array(cnt[:], dtype=np.int64)
+
+    @property
+    def n_scenes(self) -> int:
+        return len(self.scene_count)
+
+    def scene(self, array: np.ndarray, s: int) -> np.ndarray:
+        a = int(self.scene_first[s])
+        return array[a:a + int(self.scene_count[s])]
+
+    def read_scene_stats(self, s: int) -> _abi.FeStats:
+        st = _abi.FeStats()
+        check(self._lib, self._lib.fe_read_scene_stats(self.handle, s, ctypes.byref(st)),
+              "fe_read_scene_stats")
+        return st
+
+    def set_scene_params(self, s: int, sim_params: _abi.FeParams) -> None:
+        p = _abi.copy_params(sim_params)
+        check(self._lib, self._lib.fe_set_scene_params(self.handle, s, ctypes.byref(p)),
+              "fe_set_scene_params")
+
+    def scene_params(self, s: int) -> _abi.FeParams:
+        p = _abi.FeParams()
+        check(self._lib, self._lib.fe_get_scene_params(self.handle, s, ctypes.byref(p)),
+              "fe_get_scene_params")
+        return p
+
+
+class BatchSimulation(Simulation):
+    """fe_step over a batch: every scene advances one frame per call."""
+
+    def __init__(self, scene_positions, scene_params, *, scene_velocities=None, device=0):
+        self.data = BatchPhysicsData(scene_positions, scene_params,
+                                     scene_velocities=scene_velocities, device=device)
+        lib = self.data._lib
+        check(lib, lib.fe_prepare(self.data.handle), "fe_prepare")
+
+
 def sort_pairs_host(keys, values, key_bits: int = 32, algorithm: int = _abi.FE_SORT_RADIX):
     """fe_sort_pairs_host on copies of the arrays."""
     lib = load_library()

@@ -146,6 +146,51 @@ def workload(name: str) -> Workload:
     return w
 
 
+@dataclass
+class BatchWorkload:
+    """Independent dam-break scenes advanced together (fe_batch_create)."""
+    name: str
+    counts: list
+    boxes: list          # (box_min, box_max) per scene
+    viscosities: list
+    steps: int
+    seed: int = 1
+
+    def positions(self) -> list:
+        out = []
+        sp = np.float32(0.05)
+        for k, (n, (bmin, _)) in enumerate(zip(self.counts, self.boxes)):
+            nx = int(math.ceil((n / 4.0) ** (1.0 / 3.0) - 1e-9))
+            pos, _ = lattice(bmin, (nx, 2 * nx, 2 * nx), 0.025, 1000.0, sp, 0.01,
+                             seed=self.seed * 1000 + k)
+            out.append(pos[:n])
+        return out
+
+    def params(self) -> list:
+        return [dam_break_params(bmin, bmax, viscosity=float(nu))
+                for (bmin, bmax), nu in zip(self.boxes, self.viscosities)]
+
+
+def batch_workload(n_scenes: int = 64, seed: int = 1, lo: int = 4096, hi: int = 262144,
+                   fill: float = 0.25, steps: int = 500) -> BatchWorkload:
+    """The batched dam breaks: n_scenes scenes with particle counts drawn
+    log-uniform in [lo, hi] and XSPH coefficients uniform in [0.005, 0.05]
+    (one seeded stream), each a column of the 16k dam break's 1:2:2 shape
+    (nx x 2nx x 2nx lattice at spacing 0.05, cut to the drawn count) in a
+    cubic box whose volume is count * spacing^3 / fill.  Physics otherwise as
+    the 16k dam break (dt 1 ms, 4 + 4 Jacobi iterations, radix sort)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), n_scenes)).astype(np.int64)
+    counts = np.clip(counts, lo, hi)
+    nus = rng.uniform(0.005, 0.05, n_scenes)
+    boxes = []
+    for n in counts:
+        edge = float((float(n) * 0.05 ** 3 / fill) ** (1.0 / 3.0))
+        boxes.append(((0.0, 0.0, 0.0), (edge, edge, edge)))
+    return BatchWorkload(f"dam_break_batch{n_scenes}", [int(c) for c in counts], boxes,
+                         [float(v) for v in nus], steps, seed)
+
+
 def rest_density_scene():
     """rest_density_diagnostic (convergence_benchmark.rs:420-542): no jitter,
     20x20x12 lattice, r 0.02, s 0.04, h 0.08, bitonic sort (the

@@ -230,6 +230,28 @@ FE_API fe_status fe_validate_params(const fe_params* params);
 FE_API fe_status fe_create(const fe_params* params, uint32_t n, const float* pos_xyz,
                     const float* vel_xyz, int device, fe_ctx** out);
 
+/* Batched scenes: one context over n_scenes independent scenes of uneven
+ * particle counts, advanced together by every stage launch and every
+ * fe_step (one CUDA graph for all of them).  The reference runs one scene
+ * per `GpuPhysicsData` (particle.rs:137-308); this replaces n_scenes of
+ * them.  params[n_scenes] and counts[n_scenes] are per scene; pos_xyz and
+ * vel_xyz hold the scenes back to back (scene s starts at particle
+ * first_s = counts[0] + ... + counts[s-1]), and every field of
+ * fe_upload/fe_download uses the same layout.  Scenes are independent: each
+ * gets the result it would get in a context of its own, bit for bit.  All
+ * scenes must share sort_algorithm (FE_SORT_RADIX when n_scenes > 1), mode
+ * and warm_start; physics, dt, adaptive CFL, solver and tolerances are per
+ * scene.  Sum of counts <= FE_MAX_PARTICLES. */
+#define FE_MAX_SCENES 65536u
+FE_API fe_status fe_batch_create(const fe_params* params, const uint32_t* counts,
+                                 uint32_t n_scenes, const float* pos_xyz,
+                                 const float* vel_xyz, int device, fe_ctx** out);
+/* Number of scenes (1 for fe_create), and each scene's first particle and
+ * particle count (arrays of at least `capacity` entries). */
+FE_API fe_status fe_scene_count(const fe_ctx* ctx, uint32_t* out);
+FE_API fe_status fe_scene_table(const fe_ctx* ctx, uint32_t* first, uint32_t* count,
+                                uint32_t capacity);
+
 /* Frees everything owned by ctx.  NULL is accepted. */
 FE_API fe_status fe_destroy(fe_ctx* ctx);
 
@@ -237,6 +259,10 @@ FE_API fe_status fe_destroy(fe_ctx* ctx);
  * the parameter block used by later calls. */
 FE_API fe_status fe_set_params(fe_ctx* ctx, const fe_params* params);
 FE_API fe_status fe_get_params(const fe_ctx* ctx, fe_params* out);
+/* The same for one scene of a batch (fe_set_params sets every scene;
+ * fe_get_params reads scene 0). */
+FE_API fe_status fe_set_scene_params(fe_ctx* ctx, uint32_t scene, const fe_params* params);
+FE_API fe_status fe_get_scene_params(const fe_ctx* ctx, uint32_t scene, fe_params* out);
 
 /* `ComputeStep::prepare` for all passes (renderer/mod.rs:137-192): binds
  * buffers and sizes launches.  Must precede the stage calls and fe_step. */
@@ -287,6 +313,9 @@ FE_API fe_status fe_stats_pass(fe_ctx* ctx);
 /* Reads the stats of the last stats pass (host read of `stats_buffer`,
  * renderer/mod.rs:231-236).  Synchronises the context's stream. */
 FE_API fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
+/* The stats of one scene of a batch (fe_read_stats reads scene 0).  The
+ * FE_STATS_ITERATION_CAP_HIT and look-back flags are shared by all scenes. */
+FE_API fe_status fe_read_scene_stats(fe_ctx* ctx, uint32_t scene, fe_stats* out);
 
 /* ------------------------------------------------------------------------- */
 /* Whole step                                                                */
