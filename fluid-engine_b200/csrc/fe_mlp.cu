@@ -126,12 +126,24 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// SiLU with the fast exponential and division intrinsics (the network is
-// BF16; full-precision division would only cost time).
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// The hardware tanh (PTX tanh.approx.f32: one special-function-unit op,
+// about 2^-11 relative error, far below the network's BF16 rounding).
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// SiLU z * sigmoid(z) with sigmoid(z) = (1 + tanh(z / 2)) / 2, i.e.
+// s + s * tanh(s) for s = z / 2: one special-function op per activation
+// instead of an exponential and a reciprocal.
+__device__ __forceinline__ float silu(float z) {
+    const float s = 0.5f * z;
+    return s + s * tanh_hw(s);
+}
 __device__ __forceinline__ float silu_grad(float z) {
-    float s = __fdividef(1.0f, 1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
+    const float sg = 0.5f + 0.5f * tanh_hw(0.5f * z);
+    return sg * (1.0f + z * (1.0f - sg));
 }
 
 __device__ __forceinline__ void st_bf16(uint8_t* base, uint32_t off, float v) {
@@ -231,7 +243,8 @@ __device__ __forceinline__ uint32_t lane_addr8(uint32_t base, uint32_t col) {
 }
 
 // 32 accumulator columns [c0, c0 + 32) of this warp's rows -> bias + SiLU ->
-// BF16 into the K-major [128 x 64] tile.
+// BF16 into the K-major [128 x 64] tile.  Eight consecutive columns of a row
+// are 16 contiguous bytes of the canonical layout: one 16-byte store each.
 __device__ __forceinline__ void epilogue_half(uint32_t taddr, uint32_t c0, const float* bias,
                                               uint8_t* out, uint32_t row) {
 #pragma unroll
@@ -239,10 +252,17 @@ __device__ __forceinline__ void epilogue_half(uint32_t taddr, uint32_t c0, const
         float v[16];
         tmem_ld16(taddr + c0 + cc, v);
 #pragma unroll
-        for (int i = 0; i < 16; i += 2) {
-            __nv_bfloat162 two = __floats2bfloat162_rn(silu(v[i] + bias[c0 + cc + i]),
-                                                       silu(v[i + 1] + bias[c0 + cc + i + 1]));
-            *reinterpret_cast<__nv_bfloat162*>(out + off_k(row, c0 + cc + i, 64)) = two;
+        for (int g = 0; g < 16; g += 8) {
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t c = c0 + cc + g + 2 * j;
+                __nv_bfloat162 two = __floats2bfloat162_rn(silu(v[g + 2 * j] + bias[c]),
+                                                           silu(v[g + 2 * j + 1] + bias[c + 1]));
+                w[j] = *reinterpret_cast<uint32_t*>(&two);
+            }
+            *reinterpret_cast<uint4*>(out + off_k(row, c0 + cc + g, 64)) =
+                make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }

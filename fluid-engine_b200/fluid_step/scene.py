@@ -13,6 +13,9 @@ Dam-break workloads (particle-steps/s benchmarks and parity cases):
   dam_break_16k   16x32x32 lattice, s=0.05, box [0,2]^3, jitter 0.01,
                   rho0 1000, m 0.125, h 0.1, nu 0.01, dt 1 ms, K 4+4, radix
   dam_break_256k  64^3 lattice in [0,4]^3, adaptive CFL, tolerance 0.1 %
+  dam_break_256k_cfl03  the same with CFL number 0.3 instead of 0.4: with the
+                  reference's 0.4 h / v_max the plain solver's flow clumps
+                  and blows up near frame 630 of the 1000
   dam_break_1m    128x64x128 lattice in [0,8]x[0,4]x[0,8], tolerance 0.1 %
   dam_break_1m_cfl  the same scene with the adaptive CFL step of the 262k one
   dam_break_4m    256x64x256 lattice in [0,16]x[0,4]x[0,16] (the 1M scene
@@ -123,6 +126,12 @@ def workload(name: str) -> Workload:
         w.params = dam_break_params(w.box_min, w.box_max, use_cfl=True,
                                     solver=_abi.FE_SOLVER_TOLERANCE,
                                     mode=_abi.FE_MODE_FIXED)
+    elif name == "dam_break_256k_cfl03":
+        w = Workload(name, (64, 64, 64), (0.0, 0.0, 0.0), (4.0, 4.0, 4.0), 1000)
+        w.params = dam_break_params(w.box_min, w.box_max, use_cfl=True,
+                                    solver=_abi.FE_SOLVER_TOLERANCE,
+                                    mode=_abi.FE_MODE_FIXED)
+        w.params.cfl_lambda = 0.3
     elif name == "dam_break_1m":
         w = Workload(name, (128, 64, 128), (0.0, 0.0, 0.0), (8.0, 4.0, 8.0), 200)
         w.params = dam_break_params(w.box_min, w.box_max,
