@@ -662,7 +662,7 @@ def run_reference(args) -> None:
     dt = time.perf_counter() - t0
     v = pos.shape[0] * steps / dt
     out = {"impl": "reference",
-           "metric": "DFSPH particle-steps/s (plain Jacobi to 0.1% density/divergence error)",
+           "metric": "DFSPH particle-steps/s (Jacobi to 0.1% density and divergence error)",
            "value": v, "unit": "particle-steps/s", "n_gpus": world, "steps": steps,
            "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3 / steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
