@@ -29,6 +29,7 @@
 #include "fe_mlp.h"
 #include "fe_model.h"
 #include "fe_sort.h"
+#include "fe_tune.h"
 
 using namespace fe;
 
@@ -271,6 +272,10 @@ struct fe_ctx {
     LearnArgs L{};
     bool capture = false;
 
+    // tuned shapes (fe_autotune / fe_set_tuning)
+    RadixConfig radix_cfg = kRadixDefault;
+    int mlp_ctas = mlp::kInferDefaultCtasPerSm;
+
     bool learned() const { return params[0].warm_start == FE_WARM_LEARNED && model != nullptr; }
     bool carries() const { return L.carry != nullptr && (learned() || capture); }
 
@@ -332,7 +337,7 @@ fe_status rec_check(cudaError_t e, const char* what) {
 fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
     Bufs B = c->B;
     const bool radix = c->sort_algorithm() == FE_SORT_RADIX;
-    uint32_t passes = radix_passes(c->key_bits);
+    uint32_t passes = radix_passes(c->key_bits, c->radix_cfg.digit_bits);
     // Radix ping-pongs through tmp; hashing into tmp when the pass count is
     // odd leaves the sorted entries in keys/vals.
     Bufs H = B;
@@ -346,7 +351,7 @@ fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
         bool in_tmp = false;
         REC(radix_sort(L, H.keys, H.vals, H.keys == B.keys ? c->tmp_keys : B.keys,
                        H.vals == B.vals ? c->tmp_vals : B.vals, c->n, c->key_bits,
-                       c->sort_scratch, &B.G->flags, &in_tmp));
+                       c->sort_scratch, &B.G->flags, &in_tmp, c->radix_cfg));
     } else {
         REC(bitonic_sort(L, B.keys, B.vals, c->T));
     }
@@ -421,7 +426,7 @@ fe_status rec_mlp(fe_ctx* c, Recorder& R) {
     mlp::KernelLaunch KL;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    REC(mlp::infer_launch(c->n, sms, &KL));
+    REC(mlp::infer_launch(c->n, sms, &KL, c->mlp_ctas));
     mlp::Params P = c->model->params();
     const __nv_bfloat16* X = static_cast<const __nv_bfloat16*>(c->L.xb);
     float* out = c->L.out;
@@ -803,7 +808,7 @@ fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n
     B.n_chunks = nchunks;
     B.n_scenes = n_scenes;
     uint4* chunks_d = nullptr;
-    const size_t scratch_words = radix_scratch_words(n, c->key_bits);
+    const size_t scratch_words = radix_scratch_words_any(n, c->key_bits);
     if ((s = dev_alloc(c, &B.pos_a, n)) || (s = dev_alloc(c, &B.pos_b, n)) ||
         (s = dev_alloc(c, &B.rec, 2 * (size_t)n)) ||
         (s = dev_alloc(c, &B.vel_a, n)) || (s = dev_alloc(c, &B.vel_b, n)) ||
@@ -1286,8 +1291,11 @@ std::mutex g_sort_mutex;
 SortScratch g_sort[16];
 }  // namespace
 
-fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
-                        int algorithm, void* stream_ptr) {
+namespace {
+
+// The standalone sort; `forced` overrides the tuned (or default) radix shape.
+fe_status sort_pairs_impl(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
+                          int algorithm, void* stream_ptr, const RadixConfig* forced) {
     if ((!keys || !vals) && n > 0) {
         set_error("NULL keys or values");
         return FE_ERR_INVALID_ARGUMENT;
@@ -1325,7 +1333,13 @@ fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key
     }
     std::lock_guard<std::mutex> lock(g_sort_mutex);
     SortScratch& S = g_sort[dev];
-    size_t words = radix_scratch_words(n, key_bits ? key_bits : 32);
+    const uint32_t kb = key_bits ? key_bits : 32;
+    RadixConfig cfg = kRadixDefault;
+    if (forced)
+        cfg = *forced;
+    else
+        sort_tuning_lookup(dev, n, kb, &cfg);
+    size_t words = radix_scratch_words(n, kb, cfg);
     if (S.cap < n || S.nwords < words) {
         if (S.done) FE_CUDA(cudaEventSynchronize(S.done));
         cudaFree(S.tk);
@@ -1347,14 +1361,176 @@ fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key
         FE_CUDA(cudaStreamWaitEvent(stream, S.done, 0));
     }
     bool in_tmp = false;
-    REC(radix_sort(L, keys, vals, S.tk, S.tv, n, key_bits ? key_bits : 32, S.words, S.flags,
-                   &in_tmp));
+    REC(radix_sort(L, keys, vals, S.tk, S.tv, n, kb, S.words, S.flags, &in_tmp, cfg));
     if (in_tmp) {
         FE_CUDA(cudaMemcpyAsync(keys, S.tk, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream));
         FE_CUDA(cudaMemcpyAsync(vals, S.tv, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream));
     }
     FE_CUDA(cudaEventRecord(S.done, stream));
     return FE_OK;
+}
+
+}  // namespace
+
+fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
+                        int algorithm, void* stream_ptr) {
+    return sort_pairs_impl(keys, vals, n, key_bits, algorithm, stream_ptr, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Autotuning (fe_tune.cu).
+// ---------------------------------------------------------------------------
+namespace {
+
+void fill_radix_report(fe_tune_report* r, const float* ms) {
+    r->radix_candidates = kRadixCandidateCount;
+    for (int k = 0; k < kRadixCandidateCount; ++k) {
+        r->radix_digit_bits[k] = kRadixCandidates[k].digit_bits;
+        r->radix_items[k] = kRadixCandidates[k].items;
+        r->radix_ms[k] = ms[k];
+    }
+}
+
+}  // namespace
+
+fe_status fe_autotune(fe_ctx* c, fe_tune_report* report) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    fe_tune_report r;
+    std::memset(&r, 0, sizeof r);
+    // The sort is tuned on this context's own keys: the hashes of the
+    // current positions (nearly sorted after the first frame), not random
+    // keys, into temporary arrays.
+    uint32_t *hk = nullptr, *hv = nullptr;
+    if (cudaMalloc(&hk, (size_t)c->n * 4) != cudaSuccess ||
+        cudaMalloc(&hv, (size_t)c->n * 4) != cudaSuccess) {
+        cudaFree(hk);
+        set_error("cudaMalloc of the tuning keys failed");
+        return FE_ERR_OUT_OF_MEMORY;
+    }
+    Bufs H = c->B;
+    H.keys = hk;
+    H.vals = hv;
+    k_hash<<<chunk_grid(c), kBlock, 0, c->stream>>>(H);
+    cudaError_t e = cudaGetLastError();
+    float ms[kRadixCandidateCount] = {};
+    RadixConfig best = kRadixDefault;
+    if (e == cudaSuccess) e = tune_radix(c->stream, hk, hv, c->n, c->key_bits, 7, &best, ms);
+    cudaFree(hk);
+    cudaFree(hv);
+    if (e != cudaSuccess) {
+        set_error("radix tuning: %s", cudaGetErrorString(e));
+        return FE_ERR_CUDA;
+    }
+    fill_radix_report(&r, ms);
+    int ctas = c->mlp_ctas;
+    if (c->model && c->L.xb && c->L.out) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        float mms[kMlpCtaCandidates] = {};
+        e = tune_mlp(c->stream, c->model->params(), static_cast<const __nv_bfloat16*>(c->L.xb),
+                     c->L.out, c->n, &c->B.G->flags, sms, 7, &ctas, mms);
+        if (e != cudaSuccess) {
+            set_error("network tuning: %s", cudaGetErrorString(e));
+            return FE_ERR_CUDA;
+        }
+        r.mlp_candidates = kMlpCtaCandidates;
+        for (int k = 0; k < kMlpCtaCandidates; ++k) {
+            r.mlp_ctas_per_sm[k] = (uint32_t)kMlpCtaChoices[k];
+            r.mlp_ms[k] = mms[k];
+        }
+    }
+    drop_graphs(c);  // recorded frames hold the previous shapes
+    c->radix_cfg = best;
+    c->mlp_ctas = ctas;
+    r.chosen.radix_digit_bits = best.digit_bits;
+    r.chosen.radix_items = best.items;
+    r.chosen.mlp_ctas_per_sm = (uint32_t)ctas;
+    if (report) *report = r;
+    return FE_OK;
+}
+
+fe_status fe_get_tuning(const fe_ctx* c, fe_tuning* out) {
+    if (!c || !out) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    std::memset(out, 0, sizeof *out);
+    out->radix_digit_bits = c->radix_cfg.digit_bits;
+    out->radix_items = c->radix_cfg.items;
+    out->mlp_ctas_per_sm = (uint32_t)c->mlp_ctas;
+    return FE_OK;
+}
+
+fe_status fe_set_tuning(fe_ctx* c, const fe_tuning* t) {
+    if (!c || !t) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    RadixConfig cfg{t->radix_digit_bits, t->radix_items};
+    if (!radix_config_valid(cfg)) {
+        set_error("radix shape %u-bit digits x %u keys per thread is not a candidate",
+                  t->radix_digit_bits, t->radix_items);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (t->mlp_ctas_per_sm < 1 || t->mlp_ctas_per_sm > (uint32_t)mlp::kInferMaxCtasPerSm) {
+        set_error("mlp_ctas_per_sm %u outside 1..%d", t->mlp_ctas_per_sm, mlp::kInferMaxCtasPerSm);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    drop_graphs(c);
+    c->radix_cfg = cfg;
+    c->mlp_ctas = (int)t->mlp_ctas_per_sm;
+    return FE_OK;
+}
+
+fe_status fe_autotune_sort(const uint32_t* keys, const uint32_t* vals, uint32_t n,
+                           uint32_t key_bits, fe_tune_report* report) {
+    if ((!keys || !vals) && n > 0) {
+        set_error("NULL keys or values");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (key_bits > 32) {
+        set_error("key_bits %u above 32", key_bits);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    const uint32_t kb = key_bits ? key_bits : 32;
+    int dev = 0;
+    FE_CUDA(cudaGetDevice(&dev));
+    cudaStream_t st;
+    FE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    float ms[kRadixCandidateCount] = {};
+    RadixConfig best = kRadixDefault;
+    cudaError_t e = tune_radix(st, keys, vals, n, kb, 7, &best, ms);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) {
+        set_error("radix tuning: %s", cudaGetErrorString(e));
+        return FE_ERR_CUDA;
+    }
+    sort_tuning_store(dev, n, kb, best);
+    if (report) {
+        std::memset(report, 0, sizeof *report);
+        fill_radix_report(report, ms);
+        report->chosen.radix_digit_bits = best.digit_bits;
+        report->chosen.radix_items = best.items;
+        report->chosen.mlp_ctas_per_sm = (uint32_t)mlp::kInferDefaultCtasPerSm;
+    }
+    return FE_OK;
+}
+
+fe_status fe_sort_pairs_config(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
+                               uint32_t digit_bits, uint32_t items, void* stream) {
+    RadixConfig cfg{digit_bits, items};
+    if (!radix_config_valid(cfg)) {
+        set_error("radix shape %u-bit digits x %u keys per thread is not a candidate",
+                  digit_bits, items);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    return sort_pairs_impl(keys, vals, n, key_bits, FE_SORT_RADIX, stream, &cfg);
 }
 
 fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,

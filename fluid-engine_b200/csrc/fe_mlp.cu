@@ -654,13 +654,15 @@ __global__ void k_adam(float* __restrict__ master, float* __restrict__ grad, flo
 size_t infer_smem_bytes() { return sizeof(InferSmem) + 1024; }
 size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
 
-cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out) {
+cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out, int ctas_per_sm) {
     size_t smem = infer_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
+    if (ctas_per_sm < 1 || ctas_per_sm > kInferMaxCtasPerSm) return cudaErrorInvalidValue;
     uint32_t tiles = (n + kTile - 1) / kTile;
-    uint32_t grid = tiles < (uint32_t)(num_sms * 6) ? tiles : (uint32_t)(num_sms * 6);
+    const uint32_t cap = (uint32_t)(num_sms * ctas_per_sm);
+    uint32_t grid = tiles < cap ? tiles : cap;
     out->func = (const void*)k_mlp_infer;
     out->grid = dim3(grid > 0 ? grid : 1);
     out->block = dim3(kInferThreads);
@@ -669,10 +671,10 @@ cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out) {
 }
 
 cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t n,
-                  uint32_t* error_flags, cudaStream_t stream, int num_sms) {
+                  uint32_t* error_flags, cudaStream_t stream, int num_sms, int ctas_per_sm) {
     if (n == 0) return cudaSuccess;
     KernelLaunch L;
-    cudaError_t e = infer_launch(n, num_sms, &L);
+    cudaError_t e = infer_launch(n, num_sms, &L, ctas_per_sm);
     if (e != cudaSuccess) return e;
     k_mlp_infer<<<L.grid, L.block, L.smem, stream>>>(P, X, out, n, error_flags);
     return cudaGetLastError();

@@ -48,12 +48,19 @@ struct KernelLaunch {
     dim3 grid, block;
     size_t smem;
 };
-cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out);
+// Inference grid: min(tiles, num_sms * ctas_per_sm) blocks of 256 threads
+// looping over 128-row tiles.  Shared memory and registers allow up to
+// kInferMaxCtasPerSm blocks per SM.
+constexpr int kInferDefaultCtasPerSm = 6;
+constexpr int kInferMaxCtasPerSm = 6;
+cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out,
+                         int ctas_per_sm = kInferDefaultCtasPerSm);
 size_t train_smem_bytes();
 
 // out[i][0..1] for the BF16 rows X[i][0..15], i < n.
 cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t n,
-                  uint32_t* error_flags, cudaStream_t stream, int num_sms);
+                  uint32_t* error_flags, cudaStream_t stream, int num_sms,
+                  int ctas_per_sm = kInferDefaultCtasPerSm);
 
 // Adds d(loss)/d(params) of the mean squared error over the n samples to G
 // (G must be zeroed by the caller; Adam zeroes it after each step).

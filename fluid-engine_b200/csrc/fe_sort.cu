@@ -1,14 +1,17 @@
 // fe_sort.cu — key/value sorts for the neighbour search.
 //
-// Radix: stable LSD radix sort with 8-bit digits, ceil(key_bits / 8) passes.
-// The reference runs count -> single-workgroup scan -> scatter per pass
-// (radix_count.comp, radix_scan.comp, radix_reorder.comp; 12 dispatches for
-// 4 passes).  Here one histogram kernel counts all passes' digits in a single
-// read of the keys, and each pass is ONE kernel ("onesweep"): a block takes
-// the next tile of 4096 keys from an atomic ticket, ranks them stably with
-// warp match/ballot, publishes its per-digit counts and looks back over the
+// Radix: stable LSD radix sort with b-bit digits (b = 8 or 10),
+// ceil(key_bits / b) passes.  The reference runs count -> single-workgroup
+// scan -> scatter per pass with 8-bit digits (radix_count.comp,
+// radix_scan.comp, radix_reorder.comp; 12 dispatches for 4 passes).  Here one
+// histogram kernel counts all passes' digits in a single read of the keys,
+// and each pass is ONE kernel ("onesweep"): a block takes the next tile of
+// 256 x items keys from an atomic ticket, ranks them stably with warp
+// match/ballot, publishes its per-digit counts and looks back over the
 // preceding tiles' published counts (decoupled look-back) to find where each
 // digit of the tile goes, then writes the tile out through shared memory.
+// Digit width and keys per thread are template parameters (RadixConfig); the
+// result does not depend on them.
 // The permutation equals the reference's stable sort (cpu_radix_sort,
 // sorter.rs:465-559).  Every wait on another block is bounded: after
 // kMaxSpins polls the block records FE_STATS_LOOKBACK_TIMEOUT and moves on,
@@ -29,8 +32,6 @@ namespace fe {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096 keys per tile
 constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
@@ -77,44 +78,66 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 }
 
 // One read of the keys: digit histograms of all passes.
+template <int kBits>
 __global__ void __launch_bounds__(kThreads) k_radix_hist(const uint32_t* __restrict__ keys,
                                                          uint32_t n, int passes,
                                                          uint32_t* __restrict__ hist) {
-    __shared__ uint32_t s_hist[4][256];
-    for (int t = threadIdx.x; t < 4 * 256; t += kThreads) (&s_hist[0][0])[t] = 0;
+    constexpr uint32_t kDig = 1u << kBits;
+    __shared__ uint32_t s_hist[4][kDig];
+    for (uint32_t t = threadIdx.x; t < 4 * kDig; t += kThreads) (&s_hist[0][0])[t] = 0;
     __syncthreads();
     const uint32_t stride = gridDim.x * kThreads;
     for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
         uint32_t k = keys[i];
-        for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(k >> (8 * p)) & 0xFF], 1u);
+        for (int p = 0; p < passes; ++p) atomicAdd(&s_hist[p][(k >> (kBits * p)) & (kDig - 1)], 1u);
     }
     __syncthreads();
-    for (int p = 0; p < passes; ++p) {
-        uint32_t c = s_hist[p][threadIdx.x];
-        if (c) atomicAdd(&hist[p * 256 + threadIdx.x], c);
-    }
+    for (int p = 0; p < passes; ++p)
+        for (uint32_t d = threadIdx.x; d < kDig; d += kThreads) {
+            uint32_t c = s_hist[p][d];
+            if (c) atomicAdd(&hist[p * kDig + d], c);
+        }
 }
 
-// One onesweep pass (see the file comment).
-__global__ void __launch_bounds__(kThreads) k_radix_pass(
+// Shared-memory bytes of one pass block.
+template <int kBits, int kItems>
+constexpr size_t pass_smem_bytes() {
+    return 4u * ((size_t)2 * kThreads * kItems + (size_t)kWarps * (1u << kBits) +
+                 2u * (1u << kBits) + kWarps + 1);
+}
+
+// One onesweep pass (see the file comment) with kBits-bit digits and kItems
+// keys per thread; thread t owns digits [t * kDpt, (t + 1) * kDpt) in the
+// digit phases.
+template <int kBits, int kItems>
+constexpr int pass_min_blocks() {
+    return (kBits > 8 && kItems > 8) ? 2 : 3;
+}
+
+template <int kBits, int kItems>
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<kBits, kItems>()) k_radix_pass(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
     const uint32_t* __restrict__ hist, uint32_t* __restrict__ status,
     uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ error_flags) {
-    __shared__ uint32_t s_keys[kTile];
-    __shared__ uint32_t s_vals[kTile];
-    __shared__ uint32_t s_whist[kWarps][256];
-    __shared__ uint32_t s_tile_start[256];
-    __shared__ uint32_t s_dest_base[256];
-    __shared__ uint32_t s_scan[kWarps];
-    __shared__ uint32_t s_tile;
+    constexpr uint32_t kDig = 1u << kBits;
+    constexpr uint32_t kMask = kDig - 1;
+    constexpr int kDpt = (int)(kDig / kThreads);
+    constexpr int kTile = kThreads * kItems;
+    extern __shared__ __align__(16) uint32_t smem[];
+    uint32_t* s_keys = smem;
+    uint32_t* s_vals = s_keys + kTile;
+    uint32_t* s_whist = s_vals + kTile;            // [kWarps][kDig]
+    uint32_t* s_tile_start = s_whist + kWarps * kDig;
+    uint32_t* s_dest_base = s_tile_start + kDig;
+    uint32_t* s_scan = s_dest_base + kDig;
+    uint32_t* s_tile = s_scan + kWarps;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int d_self = threadIdx.x;  // digit owned by this thread in the digit phases
-    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-    for (int t = threadIdx.x; t < kWarps * 256; t += kThreads) (&s_whist[0][0])[t] = 0;
+    if (threadIdx.x == 0) *s_tile = atomicAdd(tile_counter, 1u);
+    for (uint32_t t = threadIdx.x; t < kWarps * kDig; t += kThreads) s_whist[t] = 0;
     __syncthreads();
-    const uint32_t tile = s_tile;
+    const uint32_t tile = *s_tile;
     const uint32_t base = tile * kTile;
 
     // Load (warp-striped: item it of lane l at warp*32*kItems + it*32 + l).
@@ -129,13 +152,13 @@ __global__ void __launch_bounds__(kThreads) k_radix_pass(
     // Stable rank within the warp, items in position order.
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-        uint32_t d = (key[it] >> shift) & 0xFF;
+        uint32_t d = (key[it] >> shift) & kMask;
         uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
         int leader = __ffs(peers) - 1;
         uint32_t before = 0;
         if (lane == leader) {
-            before = s_whist[warp][d];
-            s_whist[warp][d] = before + __popc(peers);
+            before = s_whist[warp * kDig + d];
+            s_whist[warp * kDig + d] = before + __popc(peers);
         }
         before = __shfl_sync(0xFFFFFFFFu, before, leader);
         rank[it] = before + __popc(peers & lanemask_lt());
@@ -144,53 +167,68 @@ __global__ void __launch_bounds__(kThreads) k_radix_pass(
     __syncthreads();
 
     // Digit phase: warp offsets, tile digit counts and starts.
-    uint32_t count = 0;
-    for (int w = 0; w < kWarps; ++w) {
-        uint32_t c = s_whist[w][d_self];
-        s_whist[w][d_self] = count;
-        count += c;
+    const uint32_t d0 = threadIdx.x * kDpt;
+    uint32_t count[kDpt];
+    uint32_t tsum = 0, hsum = 0, hv[kDpt];
+#pragma unroll
+    for (int j = 0; j < kDpt; ++j) {
+        uint32_t c = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            uint32_t v = s_whist[w * kDig + d0 + j];
+            s_whist[w * kDig + d0 + j] = c;
+            c += v;
+        }
+        count[j] = c;
+        tsum += c;
+        hv[j] = hist[d0 + j];
+        hsum += hv[j];
     }
     uint32_t total;
-    uint32_t tile_start = block_exclusive_scan(count, s_scan, &total);
-    s_tile_start[d_self] = tile_start;
+    uint32_t tile_prefix = block_exclusive_scan(tsum, s_scan, &total);
+    uint32_t gprefix = block_exclusive_scan(hsum, s_scan, &total);
 
-    // Global digit base: exclusive scan of this pass's histogram.
-    uint32_t gbase = block_exclusive_scan(hist[d_self], s_scan, &total);
-
-    // Decoupled look-back for digit d_self.
-    uint32_t* my = status + (size_t)tile * 256 + d_self;
-    uint32_t excl = 0;
-    if (tile == 0) {
-        atomicExch(my, kFlagInc | count);
-    } else {
-        atomicExch(my, kFlagAgg | count);
-        int pred = (int)tile - 1;
-        int spins = 0;
-        while (pred >= 0) {
-            uint32_t v = ld_volatile(status + (size_t)pred * 256 + d_self);
-            uint32_t flag = v & ~kValueMask;
-            if (flag == 0) {
-                if (++spins > kMaxSpins) {
-                    atomicOr(error_flags, 0x4u);
-                    break;
+    // Publish this tile's per-digit counts before looking back, so that later
+    // tiles can proceed.
+#pragma unroll
+    for (int j = 0; j < kDpt; ++j)
+        atomicExch(status + (size_t)tile * kDig + d0 + j, (tile == 0 ? kFlagInc : kFlagAgg) | count[j]);
+    uint32_t tstart = tile_prefix, gstart = gprefix;
+#pragma unroll
+    for (int j = 0; j < kDpt; ++j) {
+        const uint32_t d = d0 + j;
+        uint32_t excl = 0;
+        if (tile > 0) {
+            int pred = (int)tile - 1;
+            int spins = 0;
+            while (pred >= 0) {
+                uint32_t v = ld_volatile(status + (size_t)pred * kDig + d);
+                uint32_t flag = v & ~kValueMask;
+                if (flag == 0) {
+                    if (++spins > kMaxSpins) {
+                        atomicOr(error_flags, 0x4u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
                 }
-                __nanosleep(32);
-                continue;
+                excl += v & kValueMask;
+                if (flag == kFlagInc) break;
+                --pred;
             }
-            excl += v & kValueMask;
-            if (flag == kFlagInc) break;
-            --pred;
+            atomicExch(status + (size_t)tile * kDig + d, kFlagInc | (excl + count[j]));
         }
-        atomicExch(my, kFlagInc | (excl + count));
+        s_tile_start[d] = tstart;
+        s_dest_base[d] = gstart + excl - tstart;
+        tstart += count[j];
+        gstart += hv[j];
     }
-    s_dest_base[d_self] = gbase + excl - tile_start;
     __syncthreads();
 
     // Scatter into the tile-sorted order in shared memory.
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-        uint32_t d = (key[it] >> shift) & 0xFF;
-        uint32_t q = s_tile_start[d] + s_whist[warp][d] + rank[it];
+        uint32_t d = (key[it] >> shift) & kMask;
+        uint32_t q = s_tile_start[d] + s_whist[warp * kDig + d] + rank[it];
         s_keys[q] = key[it];
         s_vals[q] = val[it];
     }
@@ -201,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_radix_pass(
     const uint32_t valid = n - base < (uint32_t)kTile ? n - base : (uint32_t)kTile;
     for (uint32_t q = threadIdx.x; q < valid; q += kThreads) {
         uint32_t k = s_keys[q];
-        uint32_t dest = s_dest_base[(k >> shift) & 0xFF] + q;
+        uint32_t dest = s_dest_base[(k >> shift) & kMask] + q;
         if (dest < n) {  // always true unless a look-back wait gave up
             keys_out[dest] = k;
             vals_out[dest] = s_vals[q];
@@ -270,45 +308,101 @@ __global__ void __launch_bounds__(1024) k_bitonic_local(uint32_t* keys, uint32_t
 
 }  // namespace
 
-uint32_t radix_passes(uint32_t key_bits) {
-    if (key_bits == 0 || key_bits > 32) key_bits = 32;
-    return (key_bits + 7) / 8;
+const RadixConfig kRadixCandidates[kRadixCandidateCount] = {
+    {8, 4}, {8, 8}, {8, 16}, {10, 8}, {10, 16}};
+
+bool radix_config_valid(RadixConfig c) {
+    for (const RadixConfig& k : kRadixCandidates)
+        if (k.digit_bits == c.digit_bits && k.items == c.items) return true;
+    return false;
 }
 
-size_t radix_scratch_words(uint32_t n, uint32_t key_bits) {
-    uint32_t passes = radix_passes(key_bits);
-    size_t tiles = (n + kTile - 1) / kTile;
-    // hist[passes*256] + counters[passes] (padded to 8) + status[passes*tiles*256]
-    return (size_t)passes * 256 + 8 + (size_t)passes * tiles * 256;
+uint32_t radix_passes(uint32_t key_bits, uint32_t digit_bits) {
+    if (key_bits == 0 || key_bits > 32) key_bits = 32;
+    return (key_bits + digit_bits - 1) / digit_bits;
 }
+
+size_t radix_scratch_words(uint32_t n, uint32_t key_bits, RadixConfig cfg) {
+    const uint32_t passes = radix_passes(key_bits, cfg.digit_bits);
+    const size_t dig = (size_t)1 << cfg.digit_bits;
+    const size_t tile = (size_t)kThreads * cfg.items;
+    const size_t tiles = (n + tile - 1) / tile;
+    // hist[passes*dig] + counters[passes] (padded to 8) + status[passes*tiles*dig]
+    return (size_t)passes * dig + 8 + (size_t)passes * tiles * dig;
+}
+
+size_t radix_scratch_words_any(uint32_t n, uint32_t key_bits) {
+    size_t w = 0;
+    for (const RadixConfig& c : kRadixCandidates) {
+        size_t x = radix_scratch_words(n, key_bits, c);
+        w = x > w ? x : w;
+    }
+    return w;
+}
+
+namespace {
+
+struct PassKernel {
+    const void* pass;
+    const void* hist;
+    size_t smem;
+};
+
+template <int kBits, int kItems>
+PassKernel pass_kernel() {
+    return {(const void*)k_radix_pass<kBits, kItems>, (const void*)k_radix_hist<kBits>,
+            pass_smem_bytes<kBits, kItems>()};
+}
+
+bool select_kernel(RadixConfig c, PassKernel* out) {
+    if (c.digit_bits == 8 && c.items == 4) *out = pass_kernel<8, 4>();
+    else if (c.digit_bits == 8 && c.items == 8) *out = pass_kernel<8, 8>();
+    else if (c.digit_bits == 8 && c.items == 16) *out = pass_kernel<8, 16>();
+    else if (c.digit_bits == 10 && c.items == 8) *out = pass_kernel<10, 8>();
+    else if (c.digit_bits == 10 && c.items == 16) *out = pass_kernel<10, 16>();
+    else return false;
+    return true;
+}
+
+}  // namespace
 
 cudaError_t radix_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint32_t* tmp_keys,
                        uint32_t* tmp_vals, uint32_t n, uint32_t key_bits, uint32_t* scratch,
-                       uint32_t* error_flags, bool* result_in_tmp) {
+                       uint32_t* error_flags, bool* result_in_tmp, RadixConfig cfg) {
     *result_in_tmp = false;
     if (n <= 1) return cudaSuccess;
-    const uint32_t passes = radix_passes(key_bits);
-    const uint32_t tiles = (n + kTile - 1) / kTile;
+    PassKernel K;
+    if (!select_kernel(cfg, &K)) return cudaErrorInvalidValue;
+    if (K.smem > 48 * 1024) {
+        // Opt-in above the default 48 KB; applies to the current device.
+        cudaError_t a = cudaFuncSetAttribute(K.pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)K.smem);
+        if (a != cudaSuccess) return a;
+    }
+    const uint32_t passes = radix_passes(key_bits, cfg.digit_bits);
+    const uint32_t dig = 1u << cfg.digit_bits;
+    const uint32_t tile = (uint32_t)kThreads * cfg.items;
+    const uint32_t tiles = (n + tile - 1) / tile;
     uint32_t* hist = scratch;
-    uint32_t* counters = scratch + passes * 256;
+    uint32_t* counters = scratch + passes * dig;
     uint32_t* status = counters + 8;
-    cudaError_t e = L.fill(scratch, 0u, radix_scratch_words(n, key_bits));
+    cudaError_t e = L.fill(scratch, 0u, radix_scratch_words(n, key_bits, cfg));
     if (e != cudaSuccess) return e;
-    uint32_t hist_blocks = tiles < 4 * 148u ? tiles : 4 * 148u;
+    uint32_t hist_tiles = (n + 4095) / 4096;
+    uint32_t hist_blocks = hist_tiles < 4 * 148u ? hist_tiles : 4 * 148u;
     int passes_i = (int)passes;
-    e = L.launch((const void*)k_radix_hist, dim3(hist_blocks), dim3(kThreads), 0,
-                 {(const void*)&keys, &n, &passes_i, &hist});
+    e = L.launch(K.hist, dim3(hist_blocks), dim3(kThreads), 0, {(const void*)&keys, &n, &passes_i, &hist});
     if (e != cudaSuccess) return e;
     uint32_t* src_k = keys;
     uint32_t* src_v = vals;
     uint32_t* dst_k = tmp_keys;
     uint32_t* dst_v = tmp_vals;
     for (uint32_t p = 0; p < passes; ++p) {
-        int shift = 8 * p;
-        const uint32_t* hp = hist + p * 256;
-        uint32_t* sp = status + (size_t)p * tiles * 256;
+        int shift = (int)(cfg.digit_bits * p);
+        const uint32_t* hp = hist + p * dig;
+        uint32_t* sp = status + (size_t)p * tiles * dig;
         uint32_t* cp = counters + p;
-        e = L.launch((const void*)k_radix_pass, dim3(tiles), dim3(kThreads), 0,
+        e = L.launch(K.pass, dim3(tiles), dim3(kThreads), K.smem,
                      {&src_k, &src_v, &dst_k, &dst_v, &n, &shift, &hp, &sp, &cp, &error_flags});
         if (e != cudaSuccess) return e;
         uint32_t* tk = src_k;

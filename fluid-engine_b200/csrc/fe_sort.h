@@ -29,19 +29,36 @@ struct SortLaunch {
     }
 };
 
-// Number of 8-bit passes for keys < 2^key_bits (key_bits 0 or > 32 = 32).
-uint32_t radix_passes(uint32_t key_bits);
+// Shape of the onesweep passes: digit width in bits and keys per thread
+// (a tile is 256 threads x items keys).  Every configuration produces the
+// same stable sort; they differ in pass count, tiles in flight and shared
+// memory per block.  The autotuner (fe_tune.cu) picks one per size.
+struct RadixConfig {
+    uint32_t digit_bits;  // 8 or 10
+    uint32_t items;       // keys per thread
+};
+constexpr RadixConfig kRadixDefault{8, 16};
+constexpr int kRadixCandidateCount = 5;
+extern const RadixConfig kRadixCandidates[kRadixCandidateCount];
+bool radix_config_valid(RadixConfig c);
 
-// 32-bit words of scratch radix_sort needs for n keys.
-size_t radix_scratch_words(uint32_t n, uint32_t key_bits);
+// Number of passes for keys < 2^key_bits (key_bits 0 or > 32 = 32).
+uint32_t radix_passes(uint32_t key_bits, uint32_t digit_bits = 8);
+
+// 32-bit words of scratch radix_sort needs for n keys with configuration
+// cfg, and the most any candidate configuration needs.
+size_t radix_scratch_words(uint32_t n, uint32_t key_bits, RadixConfig cfg = kRadixDefault);
+size_t radix_scratch_words_any(uint32_t n, uint32_t key_bits);
 
 // Stable LSD radix sort of n pairs.  Ping-pongs between (keys, vals) and
 // (tmp_keys, tmp_vals); *result_in_tmp tells where the sorted pairs are
 // (true when the number of passes is odd).  error_flags gets bit 0x4 if a
-// bounded look-back wait gave up.
+// bounded look-back wait gave up.  cudaErrorInvalidValue for a
+// configuration outside kRadixCandidates.
 cudaError_t radix_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint32_t* tmp_keys,
                        uint32_t* tmp_vals, uint32_t n, uint32_t key_bits, uint32_t* scratch,
-                       uint32_t* error_flags, bool* result_in_tmp);
+                       uint32_t* error_flags, bool* result_in_tmp,
+                       RadixConfig cfg = kRadixDefault);
 
 // In-place bitonic network; n must be a power of two.
 cudaError_t bitonic_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint32_t n);

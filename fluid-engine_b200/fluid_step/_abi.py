@@ -144,6 +144,40 @@ class FeStats(Structure):
                 for name, _ in self._fields_ if name != "reserved"}
 
 
+class FeTuning(Structure):
+    """fe_tuning: the tunable shapes (none changes a result)."""
+    _fields_ = [("radix_digit_bits", c_uint32), ("radix_items", c_uint32),
+                ("mlp_ctas_per_sm", c_uint32), ("reserved", c_uint32)]
+
+
+FE_TUNE_MAX_CANDIDATES = 8
+
+
+class FeTuneReport(Structure):
+    """fe_tune_report: median time of every candidate and the choice."""
+    _fields_ = [("radix_candidates", c_uint32),
+                ("radix_digit_bits", c_uint32 * FE_TUNE_MAX_CANDIDATES),
+                ("radix_items", c_uint32 * FE_TUNE_MAX_CANDIDATES),
+                ("radix_ms", c_float * FE_TUNE_MAX_CANDIDATES),
+                ("mlp_candidates", c_uint32),
+                ("mlp_ctas_per_sm", c_uint32 * FE_TUNE_MAX_CANDIDATES),
+                ("mlp_ms", c_float * FE_TUNE_MAX_CANDIDATES),
+                ("chosen", FeTuning)]
+
+    def as_dict(self) -> dict:
+        r = {"radix": [{"digit_bits": self.radix_digit_bits[k], "items": self.radix_items[k],
+                        "ms": self.radix_ms[k]} for k in range(self.radix_candidates)],
+             "mlp": [{"ctas_per_sm": self.mlp_ctas_per_sm[k], "ms": self.mlp_ms[k]}
+                     for k in range(self.mlp_candidates)],
+             "chosen": {"radix_digit_bits": self.chosen.radix_digit_bits,
+                        "radix_items": self.chosen.radix_items,
+                        "mlp_ctas_per_sm": self.chosen.mlp_ctas_per_sm}}
+        return r
+
+
+RADIX_CANDIDATES = [(8, 4), (8, 8), (8, 16), (10, 8), (10, 16)]
+
+
 def default_params() -> FeParams:
     """Defaults of Scene::new() (scene.rs:14-86) and AppUI::new() (ui.rs:31-49).
 
@@ -243,6 +277,12 @@ SIGNATURES = {
     "fe_set_scene_params": (c_int, [CTX, c_uint32, POINTER(FeParams)]),
     "fe_get_scene_params": (c_int, [CTX, c_uint32, POINTER(FeParams)]),
     "fe_read_scene_stats": (c_int, [CTX, c_uint32, POINTER(FeStats)]),
+    "fe_autotune": (c_int, [CTX, POINTER(FeTuneReport)]),
+    "fe_get_tuning": (c_int, [CTX, POINTER(FeTuning)]),
+    "fe_set_tuning": (c_int, [CTX, POINTER(FeTuning)]),
+    "fe_autotune_sort": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, POINTER(FeTuneReport)]),
+    "fe_sort_pairs_config": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_uint32,
+                                     c_void_p]),
     "fe_set_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_get_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_prepare": (c_int, [CTX]),

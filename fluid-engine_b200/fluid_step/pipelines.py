@@ -86,6 +86,20 @@ class GpuPhysicsData:
         check(self._lib, self._lib.fe_read_stats(self.handle, ctypes.byref(st)), "fe_read_stats")
         return st
 
+    # -- autotuning (fe_autotune) -------------------------------------------
+    def autotune(self) -> _abi.FeTuneReport:
+        r = _abi.FeTuneReport()
+        check(self._lib, self._lib.fe_autotune(self.handle, ctypes.byref(r)), "fe_autotune")
+        return r
+
+    def tuning(self) -> _abi.FeTuning:
+        t = _abi.FeTuning()
+        check(self._lib, self._lib.fe_get_tuning(self.handle, ctypes.byref(t)), "fe_get_tuning")
+        return t
+
+    def set_tuning(self, t: _abi.FeTuning) -> None:
+        check(self._lib, self._lib.fe_set_tuning(self.handle, ctypes.byref(t)), "fe_set_tuning")
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self._lib.fe_destroy(self.handle)

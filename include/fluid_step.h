@@ -343,15 +343,69 @@ FE_API fe_status fe_step(fe_ctx* ctx, uint32_t n_substeps, uint32_t flags, fe_st
  * (cudaStream_t as void*, NULL = legacy default stream).  Replaces
  * `RadixSorter::execute` / `GpuSorter::execute` on an Entry buffer
  * (sorter.rs:73-115, 325-454).
- *   FE_SORT_RADIX: stable LSD radix sort, 8-bit digits, the permutation of
+ *   FE_SORT_RADIX: stable LSD radix sort, the permutation of
  *     `cpu_radix_sort` (sorter.rs:465-559).  `key_bits` (1..32) bounds the
- *     key range: keys must be < 2^key_bits; 32 sorts any keys.
+ *     key range: keys must be < 2^key_bits; 32 sorts any keys.  Digit width
+ *     and keys per thread are those fe_autotune_sort chose for this device
+ *     and size class, else 8-bit digits and 16 keys per thread; the result
+ *     does not depend on them.
  *   FE_SORT_BITONIC: the compare-exchange network of bitonic_sort.comp;
  *     n must be a power of two; not stable (same network, same result as
  *     the reference for the same input).
  * Scratch is allocated on first use per (device, size class) and kept. */
 FE_API fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
                         uint32_t key_bits, int algorithm, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Autotuning (no reference counterpart: the reference fixes its workgroup   */
+/* sizes and 8-bit digits in the shaders)                                     */
+/* ------------------------------------------------------------------------- */
+/* Tunable shapes; none of them changes a result.
+ *   radix_digit_bits, radix_items: onesweep digit width (8 or 10) and keys
+ *     per thread (4, 8, 16; the pairs (8,4) (8,8) (8,16) (10,8) (10,16)).
+ *   mlp_ctas_per_sm: blocks per SM of the learned warm start's inference
+ *     grid (1..6). */
+typedef struct fe_tuning {
+    uint32_t radix_digit_bits;
+    uint32_t radix_items;
+    uint32_t mlp_ctas_per_sm;
+    uint32_t reserved;
+} fe_tuning;
+
+#define FE_TUNE_MAX_CANDIDATES 8
+/* Median CUDA-event time of every candidate (7 timed runs after one
+ * untimed), and the choice. */
+typedef struct fe_tune_report {
+    uint32_t radix_candidates;
+    uint32_t radix_digit_bits[FE_TUNE_MAX_CANDIDATES];
+    uint32_t radix_items[FE_TUNE_MAX_CANDIDATES];
+    float radix_ms[FE_TUNE_MAX_CANDIDATES];
+    uint32_t mlp_candidates;                 /* 0: no model attached */
+    uint32_t mlp_ctas_per_sm[FE_TUNE_MAX_CANDIDATES];
+    float mlp_ms[FE_TUNE_MAX_CANDIDATES];
+    fe_tuning chosen;
+} fe_tune_report;
+
+/* Times the candidate shapes on this context's device and data (the sort on
+ * the hashes of the current positions; the network on the current feature
+ * rows when a model is attached), applies the fastest and drops the
+ * recorded frame graphs.  Synchronises the context; allocates temporary
+ * device memory.  `report` may be NULL. */
+FE_API fe_status fe_autotune(fe_ctx* ctx, fe_tune_report* report);
+/* The context's current shapes, and setting them (e.g. from a cache of
+ * earlier tuning runs).  FE_ERR_INVALID_ARGUMENT for a shape outside the
+ * candidates. */
+FE_API fe_status fe_get_tuning(const fe_ctx* ctx, fe_tuning* out);
+FE_API fe_status fe_set_tuning(fe_ctx* ctx, const fe_tuning* tuning);
+/* Tunes fe_sort_pairs for the current device and the size class of n
+ * (ceil(log2 n), key_bits) on the given device arrays, which are not
+ * modified; later fe_sort_pairs calls of that class use the choice. */
+FE_API fe_status fe_autotune_sort(const uint32_t* d_keys, const uint32_t* d_values, uint32_t n,
+                                  uint32_t key_bits, fe_tune_report* report);
+/* fe_sort_pairs (radix) with an explicit shape. */
+FE_API fe_status fe_sort_pairs_config(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
+                                      uint32_t key_bits, uint32_t digit_bits, uint32_t items,
+                                      void* stream);
 
 /* Same as fe_sort_pairs with host arrays: copies in, sorts, copies out
  * (in place). */

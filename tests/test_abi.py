@@ -113,3 +113,31 @@ def test_create_rejects_bad_input_before_device(lib):
     assert lib.fe_create(ctypes.byref(p), 1, pos, None, 0, ctypes.byref(h)) == _abi.FE_ERR_NON_FINITE
     assert lib.fe_create(ctypes.byref(p), 0, pos, None, 0, ctypes.byref(h)) == _abi.FE_ERR_INVALID_ARGUMENT
     assert lib.fe_create(ctypes.byref(p), 1, None, None, 0, ctypes.byref(h)) == _abi.FE_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("cls,cname", [(_abi.FeTuning, "fe_tuning"),
+                                       (_abi.FeTuneReport, "fe_tune_report")])
+def test_tuning_struct_layout_matches_header(cls, cname):
+    fields = [f for f, _ in cls._fields_]
+    src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){",
+           f'printf("%zu\\n", sizeof({cname}));']
+    for f in fields:
+        src.append(f'printf("{f} %zu\\n", offsetof({cname}, {f}));')
+    src.append("return 0;}")
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "probe.c")
+        open(c, "w").write("\n".join(src))
+        exe = os.path.join(d, "probe")
+        subprocess.run(["gcc", "-o", exe, c], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    assert int(out[0]) == ctypes.sizeof(cls)
+    for line in out[1:]:
+        if line:
+            name, off = line.split()
+            assert getattr(cls, name).offset == int(off), name
+
+
+def test_sort_config_rejects_non_candidates(lib):
+    # shape validation happens before any device work
+    assert lib.fe_sort_pairs_config(None, None, 0, 32, 9, 8, None) == _abi.FE_ERR_INVALID_ARGUMENT
+    assert lib.fe_sort_pairs_config(None, None, 0, 32, 8, 5, None) == _abi.FE_ERR_INVALID_ARGUMENT
