@@ -220,6 +220,14 @@ def measure_arm(args, w, params, model, world, local):
     lib, h = sim.data._lib, sim.data.handle
     if model is not None:
         _abi.check(lib, lib.fe_set_model(h, model.handle), "fe_set_model")
+    # The autotuner picks the radix shape (and the network's grid) on this
+    # context's device and data before anything is timed.
+    if args.autotune:
+        sim.step(1)          # features and keys of a real frame to tune on
+        tune_report = sim.data.autotune().as_dict()
+    else:
+        tune_report = None
+    tuning = sim.data.tuning()
     stream = torch.cuda.ExternalStream(lib.fe_get_stream(h), device=local)
     # --eager launches each frame's kernels directly (FE_STEP_NO_GRAPH); the
     # kernels and their work are the same as in the graph replay.
@@ -281,7 +289,8 @@ def measure_arm(args, w, params, model, world, local):
         if name == "neighbor_search":
             lib.fe_density_alpha(h)
     lib.fe_synchronize(h)
-    passes = int(np.ceil(np.log2(sim.data.table_size) / 8)) or 1
+    key_bits = max(1, int(np.ceil(np.log2(max(sim.data.table_size, 2)))))
+    passes = -(-key_bits // tuning.radix_digit_bits)
     fixed_mode = params.mode == _abi.FE_MODE_FIXED
     avg = type("S", (), {"density_iterations": iters_d, "divergence_iterations": iters_v})
     launches = launches_per_frame(avg, passes, fixed_mode, model is not None) * args.steps
@@ -289,7 +298,8 @@ def measure_arm(args, w, params, model, world, local):
     return {"n": n, "dev_ms": dev_ms_max, "value": n * args.steps * world / (dev_ms_max / 1e3),
             "e2e": n * args.steps * world / e2e_s, "iters": (iters_d, iters_v),
             "kern": kern, "passes": passes, "launches": int(round(launches)),
-            "clocks": clocks.summary(), "residual": (st.density_residual, st.divergence_residual)}
+            "clocks": clocks.summary(), "residual": (st.density_residual, st.divergence_residual),
+            "tuning": tune_report}
 
 
 def sort_benchmark(lib):
@@ -303,6 +313,12 @@ def sort_benchmark(lib):
     kd = torch.from_numpy(rng.integers(0, 2**32, sort_n, dtype=np.uint64).astype(np.uint32)
                           .view(np.int32)).cuda()
     vd = torch.arange(sort_n, dtype=torch.int32, device="cuda")
+    # The autotuner times every radix shape on these keys first; fe_sort_pairs
+    # then uses its choice for this size class.
+    rep = _abi.FeTuneReport()
+    _abi.check(lib, lib.fe_autotune_sort(ctypes.c_void_p(kd.data_ptr()),
+                                         ctypes.c_void_p(vd.data_ptr()), sort_n, 32,
+                                         ctypes.byref(rep)), "fe_autotune_sort")
     k2, v2 = kd.clone(), vd.clone()
     cs = torch.cuda.current_stream()
     times = []
@@ -318,7 +334,11 @@ def sort_benchmark(lib):
         if it >= 3:
             times.append(a.elapsed_time(b))
     ms = statistics.median(times)
-    return {"n": sort_n, "ms": ms, "keys_per_s": sort_n / (ms / 1e3)}
+    ch = rep.chosen
+    passes = -(-32 // ch.radix_digit_bits)
+    return {"n": sort_n, "ms": ms, "keys_per_s": sort_n / (ms / 1e3),
+            "digit_bits": ch.radix_digit_bits, "keys_per_thread": ch.radix_items,
+            "passes": passes, "tuning": rep.as_dict()["radix"]}
 
 
 def full_run(w, params, model, local, frames=None):
@@ -559,6 +579,7 @@ def run_gpu(args) -> None:
                               / (head["dev_ms"] / args.steps / 1e3) / 1e9 / peak},
             "sort": {**sort, "roofline_frac": 68 * sort["n"] / (sort["ms"] / 1e3) / 1e9 / peak},
             "gpu_launches": head["launches"],
+            "autotune": head["tuning"],
             "clocks": head["clocks"],
             "cpu_baseline": cpu,
         }
@@ -692,6 +713,8 @@ def main():
                     help="eager frames, then one launch of each hot pass (for ncu -k)")
     ap.add_argument("--eager", action="store_true",
                     help="launch frames without CUDA graphs (for profilers)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default kernel shapes instead of tuning them first")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-scene batched dam break")
     ap.add_argument("--no-full-runs", dest="full_runs", action="store_false",

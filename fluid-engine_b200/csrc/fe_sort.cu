@@ -7,7 +7,7 @@
 // histogram kernel counts all passes' digits in a single read of the keys,
 // and each pass is ONE kernel ("onesweep"): a block takes the next tile of
 // 256 x items keys from an atomic ticket, ranks them stably with warp
-// match/ballot, publishes its per-digit counts and looks back over the
+// ballots, publishes its per-digit counts and looks back over the
 // preceding tiles' published counts (decoupled look-back) to find where each
 // digit of the tile goes, then writes the tile out through shared memory.
 // Digit width and keys per thread are template parameters (RadixConfig); the
@@ -149,11 +149,18 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<kBits, kItems>()) k_
         key[it] = ok ? keys_in[pos] : 0xFFFFFFFFu;
         val[it] = ok ? vals_in[pos] : 0u;
     }
-    // Stable rank within the warp, items in position order.
+    // Stable rank within the warp, items in position order.  The lanes with
+    // the same digit are found with one ballot per digit bit (cheaper than a
+    // match instruction on this part: the ranking chain dominates the pass).
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
         uint32_t d = (key[it] >> shift) & kMask;
-        uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        uint32_t peers = 0xFFFFFFFFu;
+#pragma unroll
+        for (int b = 0; b < kBits; ++b) {
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bal : ~bal;
+        }
         int leader = __ffs(peers) - 1;
         uint32_t before = 0;
         if (lane == leader) {
@@ -198,22 +205,47 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<kBits, kItems>()) k_
         const uint32_t d = d0 + j;
         uint32_t excl = 0;
         if (tile > 0) {
+            // Look back kLook predecessors per step: their status words are
+            // loaded together, then consumed nearest first until an
+            // inclusive prefix is found; an unpublished one (flag 0) is
+            // re-polled from there.  Each step costs one memory latency
+            // instead of kLook.
+            constexpr int kLook = 8;
             int pred = (int)tile - 1;
             int spins = 0;
-            while (pred >= 0) {
-                uint32_t v = ld_volatile(status + (size_t)pred * kDig + d);
-                uint32_t flag = v & ~kValueMask;
-                if (flag == 0) {
+            bool done = false;
+            while (!done && pred >= 0) {
+                uint32_t v[kLook];
+#pragma unroll
+                for (int q = 0; q < kLook; ++q)
+                    v[q] = pred - q >= 0 ? ld_volatile(status + (size_t)(pred - q) * kDig + d)
+                                         : kFlagInc;  // below tile 0: nothing to add
+                int used = 0;
+                bool stalled = false;
+#pragma unroll
+                for (int q = 0; q < kLook; ++q) {
+                    if (done || stalled) continue;
+                    if (pred - q < 0) {
+                        done = true;
+                        continue;
+                    }
+                    const uint32_t flag = v[q] & ~kValueMask;
+                    if (flag == 0) {
+                        stalled = true;
+                        continue;
+                    }
+                    excl += v[q] & kValueMask;
+                    ++used;
+                    if (flag == kFlagInc) done = true;
+                }
+                pred -= used;
+                if (stalled && !done) {
                     if (++spins > kMaxSpins) {
                         atomicOr(error_flags, 0x4u);
                         break;
                     }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += v & kValueMask;
-                if (flag == kFlagInc) break;
-                --pred;
             }
             atomicExch(status + (size_t)tile * kDig + d, kFlagInc | (excl + count[j]));
         }
