@@ -394,6 +394,38 @@ def full_run(w, params, model, local, frames=None):
     return out
 
 
+def splat_benchmark(w, local, reps: int = 10):
+    """fe_density_splat (clear + splat of position_a into the headless
+    grid_res^3 uint32 grid) on the workload's state after 5 frames: median of
+    `reps` CUDA-event timed calls after 2 untimed."""
+    import torch
+
+    from fluid_step import _abi
+    from fluid_step.pipelines import Simulation
+    sim = Simulation(w.positions(), w.params, device=local)
+    for _ in range(5):
+        sim.step(1)
+    lib, h = sim.data._lib, sim.data.handle
+    stream = torch.cuda.ExternalStream(lib.fe_get_stream(h), device=local)
+    times = []
+    for r in range(reps + 2):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _abi.check(lib, lib.fe_density_splat(h), "fe_density_splat")
+        b.record(stream)
+        b.synchronize()
+        if r >= 2:
+            times.append(a.elapsed_time(b))
+    grid = sim.data.splat_density()
+    res = [int(v) for v in w.params.grid_res]
+    sim.close()
+    ms = statistics.median(times)
+    n = w.positions().shape[0]
+    return {"ms": ms, "particles": n, "grid_res": res, "particles_per_s": n / (ms / 1e3),
+            "taps_per_particle": 1647, "reductions_per_s": n * 1647 / (ms / 1e3),
+            "grid_sum": int(grid.astype(np.uint64).sum())}
+
+
 def run_batch(args, world, rank, local):
     """The 64 batched dam-break scenes: this rank's LPT share of the scenes in
     one batch context (no collective inside a step), W warm-up frames, then K
@@ -517,6 +549,7 @@ def run_gpu(args) -> None:
                 r["learned_over_plain"] = r["plain"]["ms_per_step"] / r["learned"]["ms_per_step"]
             runs[name] = r
     batch = run_batch(args, world, rank, local) if args.batch else None
+    splat = splat_benchmark(w, local) if args.full_runs else None
     head = arms["learned"] if "learned" in arms else arms["plain"]
     lib = _abi.load_library()
     sort = sort_benchmark(lib)
@@ -587,6 +620,8 @@ def run_gpu(args) -> None:
             out["full_runs"] = runs
         if batch:
             out["batched"] = batch
+        if splat:
+            out["density_splat"] = splat
         if "learned" in arms and "plain" in arms:
             pl = arms["plain"]
             out["plain_jacobi"] = {"value": pl["value"], "ms_per_step": pl["dev_ms"] / args.steps,

@@ -29,6 +29,7 @@
 #include "fe_mlp.h"
 #include "fe_model.h"
 #include "fe_sort.h"
+#include "fe_splat.h"
 #include "fe_tune.h"
 
 using namespace fe;
@@ -271,6 +272,13 @@ struct fe_ctx {
     fe_model* model = nullptr;       // attached, not owned
     LearnArgs L{};
     bool capture = false;
+
+    // density splat: headless grid and the non-zero taps of the splat kernel
+    uint32_t* splat_grid = nullptr;
+    size_t splat_cap = 0;          // voxels allocated
+    int splat_res[3] = {0, 0, 0};  // resolution of the last splat
+    int4* splat_taps = nullptr;
+    uint32_t splat_ntaps = 0;
 
     // tuned shapes (fe_autotune / fe_set_tuning)
     RadixConfig radix_cfg = kRadixDefault;
@@ -537,6 +545,15 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
         case FE_FIELD_ENTRY_INDEX: *dptr = c->B.vals; *elem = 4; n = c->T; break;
         case FE_FIELD_GRID_START: *dptr = c->B.cells; *elem = 4; *pitch = 8; n = c->T; break;
         case FE_FIELD_STATS: *dptr = c->B.S; *elem = 4; n = 3; break;
+        case FE_FIELD_DENSITY_GRID:
+            if (!c->splat_grid) {
+                set_error("no density grid yet: call fe_density_splat first");
+                return 0;
+            }
+            *dptr = c->splat_grid;
+            *elem = 4;
+            n = (size_t)c->splat_res[0] * c->splat_res[1] * c->splat_res[2];
+            break;
         default: return 0;
     }
     if (*pitch == 0) *pitch = *elem;
@@ -1058,6 +1075,7 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
     void* d;
     size_t elem, pitch;
     size_t need = field_bytes(c, f, &d, &elem, &pitch);
+    if (need == 0 && f == FE_FIELD_DENSITY_GRID) return FE_ERR_INVALID_ARGUMENT;
     if (need == 0 || bytes != need) {
         set_error("field %d: expected %zu bytes, got %zu", (int)f, need, bytes);
         return FE_ERR_INVALID_ARGUMENT;
@@ -1103,6 +1121,68 @@ FE_STAGE(fe_divergence_integration,
                  c->fixed_mode() ? 1 : 0));
          return FE_OK)
 FE_STAGE(fe_stats_pass, return rec_stats(c, R))
+
+// DensityTexturePipeline::execute after clear_color_image
+// (renderer/mod.rs:385-390; density_texture.rs; splat_density.comp) into the
+// context's headless grid.
+fe_status fe_density_splat(fe_ctx* c) {
+    if (!c) {
+        set_error("context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (c->B.n_scenes != 1) {
+        set_error("fe_density_splat: one grid per context; batches have one box per scene");
+        return FE_ERR_UNSUPPORTED;
+    }
+    const fe_params& p = c->params[0];
+    const int rx = p.grid_res[0], ry = p.grid_res[1], rz = p.grid_res[2];
+    if (rx < 1 || ry < 1 || rz < 1 || rx > 1024 || ry > 1024 || rz > 1024) {
+        set_error("grid_res %d x %d x %d outside 1..1024", rx, ry, rz);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    const size_t voxels = (size_t)rx * ry * rz;
+    if (voxels > c->splat_cap) {
+        uint32_t* g = nullptr;
+        fe_status s = dev_alloc(c, &g, voxels);
+        if (s != FE_OK) return s;
+        c->splat_grid = g;
+        c->splat_cap = voxels;
+    }
+    if (!c->splat_taps) {
+        // The splat's weights per voxel offset, evaluated once on the device;
+        // the non-zero ones become the tap table (x fastest).
+        constexpr int kAll = kSplatSide * kSplatSide * kSplatSide;
+        uint32_t* w = nullptr;
+        fe_status s = dev_alloc(c, &w, kAll);
+        if (s != FE_OK) return s;
+        FE_CUDA(splat_weights(w, c->stream));
+        std::vector<uint32_t> hw(kAll);
+        FE_CUDA(cudaMemcpyAsync(hw.data(), w, kAll * 4, cudaMemcpyDeviceToHost, c->stream));
+        FE_CUDA(cudaStreamSynchronize(c->stream));
+        std::vector<int4> taps;
+        for (int t = 0; t < kAll; ++t)
+            if (hw[t])
+                taps.push_back(make_int4(t % kSplatSide - kSplatRadius,
+                                         (t / kSplatSide) % kSplatSide - kSplatRadius,
+                                         t / (kSplatSide * kSplatSide) - kSplatRadius, (int)hw[t]));
+        int4* d = nullptr;
+        if ((s = dev_alloc(c, &d, taps.size()))) return s;
+        FE_CUDA(cudaMemcpy(d, taps.data(), taps.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        c->splat_taps = d;
+        c->splat_ntaps = (uint32_t)taps.size();
+    }
+    c->splat_res[0] = rx;
+    c->splat_res[1] = ry;
+    c->splat_res[2] = rz;
+    FE_CUDA(cudaMemsetAsync(c->splat_grid, 0, voxels * 4, c->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    FE_CUDA(splat(c->B.pos_a, c->n, make_float3(p.box_min[0], p.box_min[1], p.box_min[2]),
+                  make_float3(p.box_max[0], p.box_max[1], p.box_max[2]), make_int3(rx, ry, rz),
+                  c->splat_taps, c->splat_ntaps, c->splat_grid, c->stream, sms));
+    return FE_OK;
+}
 
 fe_status fe_read_stats(fe_ctx* c, fe_stats* out) {
     if (!c || !out) {

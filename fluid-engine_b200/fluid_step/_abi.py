@@ -61,11 +61,12 @@ FE_FIELD_ENTRY_HASH = 9
 FE_FIELD_ENTRY_INDEX = 10
 FE_FIELD_GRID_START = 11
 FE_FIELD_STATS = 12
+FE_FIELD_DENSITY_GRID = 13
 
 VEC4_FIELDS = {FE_FIELD_POSITION_A, FE_FIELD_POSITION_B, FE_FIELD_VELOCITY_A,
                FE_FIELD_VELOCITY_B, FE_FIELD_PRESSURE_ACCEL}
 UINT_FIELDS = {FE_FIELD_ENTRY_HASH, FE_FIELD_ENTRY_INDEX, FE_FIELD_GRID_START,
-               FE_FIELD_STATS}
+               FE_FIELD_STATS, FE_FIELD_DENSITY_GRID}
 TABLE_FIELDS = {FE_FIELD_ENTRY_HASH, FE_FIELD_ENTRY_INDEX, FE_FIELD_GRID_START}
 
 FE_STEP_INIT_NS = 0x1
@@ -283,6 +284,7 @@ SIGNATURES = {
     "fe_autotune_sort": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, POINTER(FeTuneReport)]),
     "fe_sort_pairs_config": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_uint32,
                                      c_void_p]),
+    "fe_density_splat": (c_int, [CTX]),
     "fe_set_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_get_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_prepare": (c_int, [CTX]),

@@ -86,6 +86,19 @@ class GpuPhysicsData:
         check(self._lib, self._lib.fe_read_stats(self.handle, ctypes.byref(st)), "fe_read_stats")
         return st
 
+    # -- density_texture.rs / splat_density.comp -----------------------------
+    def splat_density(self) -> np.ndarray:
+        """Clears and splats the headless density grid (fe_density_splat);
+        returns uint32[res_z][res_y][res_x]."""
+        check(self._lib, self._lib.fe_density_splat(self.handle), "fe_density_splat")
+        p = self.current_params()
+        rx, ry, rz = (int(v) for v in p.grid_res)
+        out = np.empty((rz, ry, rx), dtype=np.uint32)
+        check(self._lib, self._lib.fe_download(self.handle, _abi.FE_FIELD_DENSITY_GRID,
+                                               out.ctypes.data_as(ctypes.c_void_p), out.nbytes),
+              "fe_download(density grid)")
+        return out
+
     # -- autotuning (fe_autotune) -------------------------------------------
     def autotune(self) -> _abi.FeTuneReport:
         r = _abi.FeTuneReport()

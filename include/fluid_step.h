@@ -188,7 +188,9 @@ typedef enum fe_field {
     FE_FIELD_ENTRY_INDEX = 10,  /* uint32[T] grid_entries[].index            */
     FE_FIELD_GRID_START = 11,   /* uint32[T]                                 */
     FE_FIELD_STATS = 12,        /* uint32[3] stats_buffer                    */
-    FE_FIELD_COUNT = 13
+    FE_FIELD_DENSITY_GRID = 13, /* uint32[res_z][res_y][res_x] of the last
+                                   fe_density_splat (download only)          */
+    FE_FIELD_COUNT = 14
 } fe_field;
 
 /* Step flags for fe_step. */
@@ -309,6 +311,15 @@ FE_API fe_status fe_divergence_source(fe_ctx* ctx);
 FE_API fe_status fe_divergence_integration(fe_ctx* ctx);
 /* StatsPipeline::execute (stats_pipeline.rs:54-66): fill(0) + stats.comp. */
 FE_API fe_status fe_stats_pass(fe_ctx* ctx);
+
+/* DensityTexturePipeline::execute after its clear_color_image
+ * (renderer/mod.rs:385-390; density_texture.rs:29-77; splat_density.comp):
+ * clears the context's headless uint32 voxel grid of params.grid_res and
+ * splats position_a into it, exactly (integer weights, order-independent
+ * sums).  The reference's R32_UINT 3D image becomes a device buffer read with
+ * fe_download(FE_FIELD_DENSITY_GRID).  Enqueued on the context's stream;
+ * single-scene contexts only; grid_res in 1..1024 per axis. */
+FE_API fe_status fe_density_splat(fe_ctx* ctx);
 
 /* Reads the stats of the last stats pass (host read of `stats_buffer`,
  * renderer/mod.rs:231-236).  Synchronises the context's stream. */

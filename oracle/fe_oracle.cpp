@@ -988,6 +988,42 @@ int fo_sort_bitonic(uint32_t* keys, uint32_t* values, uint32_t n) {
 }
 double fo_det_sum(const double* values, size_t n) { return det_sum(values, n); }
 
+// splat_density.comp:11-51, loop by loop: every particle whose normalised
+// position uvw lies in [0, 1]^3 adds uint(200 (1 - (d/8)^2)^3) to each grid
+// voxel at offset (x, y, z), d = length(vec3(x, y, z)) < 8, from its centre
+// ivec3(uvw * grid_res).  out[res_z][res_y][res_x] is cleared first (the
+// clear_color_image of renderer/mod.rs:387-389).
+void fo_splat_density(const float* pos4, uint32_t n, const fe_params* p, uint32_t* out) {
+    const int rx = p->grid_res[0], ry = p->grid_res[1], rz = p->grid_res[2];
+    std::fill(out, out + (size_t)rx * ry * rz, 0u);
+    const int radius = 8;
+    const float r = (float)radius;
+    const float sx = p->box_max[0] - p->box_min[0], sy = p->box_max[1] - p->box_min[1],
+                sz = p->box_max[2] - p->box_min[2];
+    for (uint32_t i = 0; i < n; ++i) {
+        const float u = (pos4[4 * i] - p->box_min[0]) / sx;
+        const float v = (pos4[4 * i + 1] - p->box_min[1]) / sy;
+        const float w = (pos4[4 * i + 2] - p->box_min[2]) / sz;
+        if (u < 0.0f || v < 0.0f || w < 0.0f || u > 1.0f || v > 1.0f || w > 1.0f) continue;
+        const int cx = to_int_sat<float>(u * (float)rx), cy = to_int_sat<float>(v * (float)ry),
+                  cz = to_int_sat<float>(w * (float)rz);
+        for (int z = -radius; z <= radius; ++z)
+            for (int y = -radius; y <= radius; ++y)
+                for (int x = -radius; x <= radius; ++x) {
+                    const int X = cx + x, Y = cy + y, Z = cz + z;
+                    if (X < 0 || Y < 0 || Z < 0 || X >= rx || Y >= ry || Z >= rz) continue;
+                    const float fx = (float)x, fy = (float)y, fz = (float)z;
+                    const float dist = std::sqrt((fx * fx + fy * fy) + fz * fz);
+                    if (dist < r) {
+                        const float x_norm = dist / r;
+                        float weight = 1.0f - x_norm * x_norm;
+                        weight = (weight * weight) * weight;
+                        out[((size_t)Z * ry + Y) * rx + X] += (uint32_t)(weight * 200.0f);
+                    }
+                }
+    }
+}
+
 int fo_set_threads(int t) {
     g_threads = t;
     return nthreads();

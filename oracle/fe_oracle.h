@@ -78,6 +78,10 @@ int fo_sort_bitonic(uint32_t* keys, uint32_t* values, uint32_t n);
  * partial sums over chunks (see fe_oracle.cpp). */
 double fo_det_sum(const double* values, size_t n);
 
+/* splat_density.comp:11-51 on float4 positions pos4[n] into
+ * out[grid_res z][y][x] (cleared first). */
+void fo_splat_density(const float* pos4, uint32_t n, const fe_params* params, uint32_t* out);
+
 int fo_set_threads(int threads);
 int fo_get_threads(void);
 

@@ -52,6 +52,7 @@ def lib():
             "fo_sort_radix_parallel": (None, [c_void_p, c_void_p, c_uint32, c_uint32]),
             "fo_sort_bitonic": (c_int, [c_void_p, c_void_p, c_uint32]),
             "fo_det_sum": (c_double, [c_void_p, c_size_t]),
+            "fo_splat_density": (None, [c_void_p, c_uint32, P, c_void_p]),
             "fo_set_threads": (c_int, [c_int]),
             "fo_get_threads": (c_int, []),
         }
@@ -172,6 +173,16 @@ def sort_bitonic(keys, values):
     if lib().fo_sort_bitonic(_ptr(k), _ptr(v), k.size):
         raise ValueError("bitonic sort needs a power-of-two length")
     return k, v
+
+
+def splat_density(positions4, params) -> np.ndarray:
+    """splat_density.comp on float4 positions: uint32[res_z][res_y][res_x]."""
+    pos = np.ascontiguousarray(positions4, dtype=np.float32).reshape(-1, 4)
+    rx, ry, rz = (int(v) for v in params.grid_res)
+    out = np.empty((rz, ry, rx), dtype=np.uint32)
+    p = _abi.copy_params(params)
+    lib().fo_splat_density(_ptr(pos), pos.shape[0], ctypes.byref(p), _ptr(out))
+    return out
 
 
 def det_sum(values) -> float:

@@ -231,3 +231,30 @@ def test_stats_fixed_point(oracle_mod):
     sp = np.sqrt((vel[:, 0] * vel[:, 0] + vel[:, 1] * vel[:, 1]) + vel[:, 2] * vel[:, 2])
     assert st.max_speed == np.float32(sp.max())
     assert abs(st.avg_density_error_f64 - np.mean(np.abs(rho.astype(np.float64) - 1000.0))) < 1e-9
+
+
+def test_oracle_splat_weights_and_clipping(oracle_mod):
+    """One particle in the middle of a 32^3 grid receives the full 17^3 stencil:
+    the sum equals the sum of the shader's weights over offsets with d < 8; a
+    particle beyond box_max adds nothing."""
+    import numpy as np
+
+    from fluid_step import _abi
+    p = _abi.default_params()
+    p.box_min[:] = [0.0, 0.0, 0.0]
+    p.box_max[:] = [1.0, 1.0, 1.0]
+    p.grid_res[:] = [32, 32, 32]
+    pos = np.array([[0.5, 0.5, 0.5, 1.0], [1.5, 0.5, 0.5, 1.0]], np.float32)
+    g = oracle_mod.splat_density(pos, p)
+    total = 0
+    for z in range(-8, 9):
+        for y in range(-8, 9):
+            for x in range(-8, 9):
+                d = np.float32(np.sqrt(np.float32(np.float32(x * x + y * y) + z * z)))
+                if d < 8:
+                    xn = np.float32(d / np.float32(8))
+                    wt = np.float32(1) - xn * xn
+                    wt = np.float32(np.float32(wt * wt) * wt)
+                    total += int(np.float32(wt * np.float32(200)))
+    assert int(g.sum()) == total
+    assert g[16, 16, 16] == 200 and g[16, 16, 24] == 0
