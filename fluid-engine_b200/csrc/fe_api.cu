@@ -264,6 +264,7 @@ struct fe_ctx {
     uint32_t key_bits = 32;
     bool prepared = false;
     bool initialized = false;
+    uint32_t last_substeps = 0;  // substeps of the last fe_step (fe_stats.substeps)
     std::vector<void*> allocations;
     std::vector<GraphEntry> graphs;
     SceneState* h_state = nullptr;   // pinned
@@ -627,7 +628,7 @@ fe_status collect_stats(fe_ctx* c, fe_stats* out, uint32_t scene = 0) {
     out->divergence_iterations = S.last_iters[1];
     out->total_density_iterations = S.total_iters[0];
     out->total_divergence_iterations = S.total_iters[1];
-    out->substeps = S.substeps;
+    out->substeps = c->last_substeps;
     uint32_t flags = c->h_global->flags;  // cap hit and look-back timeout: any scene
     if (S.nonfinite) flags |= 0x8u;
     out->flags = flags;
@@ -1218,6 +1219,7 @@ fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out)
         return FE_ERR_UNSUPPORTED;
     }
     const bool init = (flags & FE_STEP_INIT_NS) || !c->initialized;
+    c->last_substeps = n_substeps;
     if (flags & FE_STEP_NO_GRAPH) {
         Recorder R = eager(c);
         s = rec_frame(c, R, n_substeps, init);

@@ -200,6 +200,18 @@ def batch_workload(n_scenes: int = 64, seed: int = 1, lo: int = 4096, hi: int = 
                          [float(v) for v in nus], steps, seed)
 
 
+def app_scene(seed: int = 0):
+    """Scene::new (core/scene.rs:14-86): a 1.0 x 2.0 x 0.8 block at spacing
+    0.04 from (-1, 1, -0.8) with jitter 0.01 in the box (-1.5, 0, -1) ..
+    (0.8, 4, 1), whose min.x wall moves with amplitude 0.3 at 0.5 Hz.
+    Returns (params, positions, (wave_amplitude, wave_frequency))."""
+    p = _abi.default_params()
+    pos, mass = generate_volume((-1.0, 1.0, -0.8), 1.0, 2.0, 0.8, 0.02, 1000.0,
+                                np.float32(0.02) * np.float32(2.0), 0.01, seed)
+    p.particle_mass = float(mass)
+    return p, pos, (0.3, 0.5)
+
+
 def rest_density_scene():
     """rest_density_diagnostic (convergence_benchmark.rs:420-542): no jitter,
     20x20x12 lattice, r 0.02, s 0.04, h 0.08, bitonic sort (the

@@ -163,6 +163,6 @@ def test_full_size_batch_advances():
     assert not (st.flags & _abi.FE_STATS_NON_FINITE)
     for s in (0, 17, 63):
         ss = sim.data.read_scene_stats(s)
-        assert ss.substeps == 3 and np.isfinite(ss.avg_density_error_f64)
+        assert ss.substeps == 1 and np.isfinite(ss.avg_density_error_f64)
         assert ss.density_iterations == 4 and ss.divergence_iterations == 4
     sim.close()
