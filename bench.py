@@ -418,12 +418,30 @@ def splat_benchmark(w, local, reps: int = 10):
             times.append(a.elapsed_time(b))
     grid = sim.data.splat_density()
     res = [int(v) for v in w.params.grid_res]
+    # the water pass over the same grid: 1920 x 1080, a camera outside the box
+    from fluid_step import camera as cm
+    sim.data.set_skybox(cm.gradient_sky(1024, 512))
+    bmin, bmax = np.asarray(w.params.box_min), np.asarray(w.params.box_max)
+    centre = (bmin + bmax) / 2
+    cam = cm.make_camera(centre + np.array([0.0, 3.0, -9.0]), centre, 1920, 1080)
+    rt = []
+    for r in range(reps + 2):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _abi.check(lib, lib.fe_raymarch(h, ctypes.byref(cam)), "fe_raymarch")
+        b.record(stream)
+        b.synchronize()
+        if r >= 2:
+            rt.append(a.elapsed_time(b))
+    img = sim.data.raymarch(cam)
     sim.close()
     ms = statistics.median(times)
     n = w.positions().shape[0]
     return {"ms": ms, "particles": n, "grid_res": res, "particles_per_s": n / (ms / 1e3),
             "taps_per_particle": 1647, "reductions_per_s": n * 1647 / (ms / 1e3),
-            "grid_sum": int(grid.astype(np.uint64).sum())}
+            "grid_sum": int(grid.astype(np.uint64).sum()),
+            "raymarch": {"width": 1920, "height": 1080, "ms": statistics.median(rt),
+                         "water_pixels": float((img[..., 3] > 0).mean())}}
 
 
 def run_batch(args, world, rank, local):

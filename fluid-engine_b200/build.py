@@ -20,7 +20,7 @@ OUT = os.path.join(HERE, "fluid_step", "libfluidstep.so")
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = ["fe_kernels.cu", "fe_sort.cu", "fe_api.cu", "fe_sort_noalloc.cu", "fe_mlp.cu", "fe_tune.cu",
-           "fe_splat.cu",
+           "fe_splat.cu", "fe_raymarch.cu",
            "fe_model.cu", "fe_learned.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true",

@@ -29,6 +29,7 @@
 #include "fe_mlp.h"
 #include "fe_model.h"
 #include "fe_sort.h"
+#include "fe_raymarch.h"
 #include "fe_splat.h"
 #include "fe_tune.h"
 
@@ -280,6 +281,14 @@ struct fe_ctx {
     int splat_res[3] = {0, 0, 0};  // resolution of the last splat
     int4* splat_taps = nullptr;
     uint32_t splat_ntaps = 0;
+
+    // raymarched image and its sky
+    float4* sky = nullptr;
+    size_t sky_cap = 0;
+    int sky_w = 0, sky_h = 0;
+    float4* image = nullptr;
+    size_t image_cap = 0;
+    int image_w = 0, image_h = 0;
 
     // tuned shapes (fe_autotune / fe_set_tuning)
     RadixConfig radix_cfg = kRadixDefault;
@@ -554,6 +563,15 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
             *dptr = c->splat_grid;
             *elem = 4;
             n = (size_t)c->splat_res[0] * c->splat_res[1] * c->splat_res[2];
+            break;
+        case FE_FIELD_IMAGE:
+            if (!c->image) {
+                set_error("no image yet: call fe_raymarch first");
+                return 0;
+            }
+            *dptr = c->image;
+            *elem = 16;
+            n = (size_t)c->image_w * c->image_h;
             break;
         default: return 0;
     }
@@ -1076,7 +1094,8 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
     void* d;
     size_t elem, pitch;
     size_t need = field_bytes(c, f, &d, &elem, &pitch);
-    if (need == 0 && f == FE_FIELD_DENSITY_GRID) return FE_ERR_INVALID_ARGUMENT;
+    if (need == 0 && (f == FE_FIELD_DENSITY_GRID || f == FE_FIELD_IMAGE))
+        return FE_ERR_INVALID_ARGUMENT;
     if (need == 0 || bytes != need) {
         set_error("field %d: expected %zu bytes, got %zu", (int)f, need, bytes);
         return FE_ERR_INVALID_ARGUMENT;
@@ -1182,6 +1201,79 @@ fe_status fe_density_splat(fe_ctx* c) {
     FE_CUDA(splat(c->B.pos_a, c->n, make_float3(p.box_min[0], p.box_min[1], p.box_min[2]),
                   make_float3(p.box_max[0], p.box_max[1], p.box_max[2]), make_int3(rx, ry, rz),
                   c->splat_taps, c->splat_ntaps, c->splat_grid, c->stream, sms));
+    return FE_OK;
+}
+
+fe_status fe_set_skybox(fe_ctx* c, const float* rgba, uint32_t width, uint32_t height) {
+    if (!c || !rgba || width == 0 || height == 0) {
+        set_error("skybox needs a context, pixels and a non-zero size");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (width > 16384 || height > 16384) {
+        set_error("skybox %u x %u above 16384", width, height);
+        return FE_ERR_CAPACITY;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    const size_t texels = (size_t)width * height;
+    if (texels > c->sky_cap) {
+        float4* p = nullptr;
+        fe_status s = dev_alloc(c, &p, texels);
+        if (s != FE_OK) return s;
+        c->sky = p;
+        c->sky_cap = texels;
+    }
+    FE_CUDA(cudaMemcpyAsync(c->sky, rgba, texels * 16, cudaMemcpyHostToDevice, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    c->sky_w = (int)width;
+    c->sky_h = (int)height;
+    return FE_OK;
+}
+
+// The water pass (water_pipeline.rs; raymarch.vert/.frag) of the last
+// fe_density_splat grid into the context's RGBA32F image.
+fe_status fe_raymarch(fe_ctx* c, const fe_camera* cam) {
+    if (!c || !cam) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (!c->splat_grid) {
+        set_error("fe_raymarch: no density grid yet (fe_density_splat first)");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (!c->sky) {
+        set_error("fe_raymarch: no skybox (fe_set_skybox first)");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (cam->width == 0 || cam->height == 0 || cam->width > 16384 || cam->height > 16384) {
+        set_error("image %u x %u outside 1..16384", cam->width, cam->height);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    const size_t pixels = (size_t)cam->width * cam->height;
+    if (pixels > c->image_cap) {
+        float4* p = nullptr;
+        fe_status s = dev_alloc(c, &p, pixels);
+        if (s != FE_OK) return s;
+        c->image = p;
+        c->image_cap = pixels;
+    }
+    c->image_w = (int)cam->width;
+    c->image_h = (int)cam->height;
+    const fe_params& p = c->params[0];
+    RaymarchArgs a;
+    a.grid = c->splat_grid;
+    a.res = make_int3(c->splat_res[0], c->splat_res[1], c->splat_res[2]);
+    a.sky = c->sky;
+    a.sky_w = c->sky_w;
+    a.sky_h = c->sky_h;
+    std::memcpy(a.inv_view_proj, cam->inv_view_proj, sizeof a.inv_view_proj);
+    a.cam = make_float3(cam->camera_pos[0], cam->camera_pos[1], cam->camera_pos[2]);
+    a.box_min = make_float3(p.box_min[0], p.box_min[1], p.box_min[2]);
+    a.box_max = make_float3(p.box_max[0], p.box_max[1], p.box_max[2]);
+    a.width = (int)cam->width;
+    a.height = (int)cam->height;
+    a.out = c->image;
+    FE_CUDA(raymarch(a, c->stream));
     return FE_OK;
 }
 

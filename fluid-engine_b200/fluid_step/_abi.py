@@ -62,6 +62,7 @@ FE_FIELD_ENTRY_INDEX = 10
 FE_FIELD_GRID_START = 11
 FE_FIELD_STATS = 12
 FE_FIELD_DENSITY_GRID = 13
+FE_FIELD_IMAGE = 14
 
 VEC4_FIELDS = {FE_FIELD_POSITION_A, FE_FIELD_POSITION_B, FE_FIELD_VELOCITY_A,
                FE_FIELD_VELOCITY_B, FE_FIELD_PRESSURE_ACCEL}
@@ -143,6 +144,13 @@ class FeStats(Structure):
     def as_dict(self) -> dict:
         return {name: (list(getattr(self, name)) if name == "reserved" else getattr(self, name))
                 for name, _ in self._fields_ if name != "reserved"}
+
+
+class FeCamera(Structure):
+    """fe_camera: column-major inverse view-projection, camera position,
+    image size."""
+    _fields_ = [("inv_view_proj", c_float * 16), ("camera_pos", c_float * 3),
+                ("width", c_uint32), ("height", c_uint32), ("reserved", c_uint32 * 3)]
 
 
 class FeTuning(Structure):
@@ -285,6 +293,8 @@ SIGNATURES = {
     "fe_sort_pairs_config": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_uint32,
                                      c_void_p]),
     "fe_density_splat": (c_int, [CTX]),
+    "fe_set_skybox": (c_int, [CTX, c_void_p, c_uint32, c_uint32]),
+    "fe_raymarch": (c_int, [CTX, POINTER(FeCamera)]),
     "fe_set_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_get_params": (c_int, [CTX, POINTER(FeParams)]),
     "fe_prepare": (c_int, [CTX]),

@@ -99,6 +99,22 @@ class GpuPhysicsData:
               "fe_download(density grid)")
         return out
 
+    # -- water pass (raymarch.frag) into a headless image ---------------------
+    def set_skybox(self, rgba) -> None:
+        """Equirectangular sky, float32[height][width][4]."""
+        a = np.ascontiguousarray(rgba, dtype=np.float32)
+        check(self._lib, self._lib.fe_set_skybox(self.handle, a.ctypes.data_as(ctypes.c_void_p),
+                                                 a.shape[1], a.shape[0]), "fe_set_skybox")
+
+    def raymarch(self, camera: _abi.FeCamera) -> np.ndarray:
+        """Renders the last splat grid; returns float32[height][width][4]."""
+        check(self._lib, self._lib.fe_raymarch(self.handle, ctypes.byref(camera)), "fe_raymarch")
+        out = np.empty((camera.height, camera.width, 4), dtype=np.float32)
+        check(self._lib, self._lib.fe_download(self.handle, _abi.FE_FIELD_IMAGE,
+                                               out.ctypes.data_as(ctypes.c_void_p), out.nbytes),
+              "fe_download(image)")
+        return out
+
     # -- autotuning (fe_autotune) -------------------------------------------
     def autotune(self) -> _abi.FeTuneReport:
         r = _abi.FeTuneReport()

@@ -190,7 +190,9 @@ typedef enum fe_field {
     FE_FIELD_STATS = 12,        /* uint32[3] stats_buffer                    */
     FE_FIELD_DENSITY_GRID = 13, /* uint32[res_z][res_y][res_x] of the last
                                    fe_density_splat (download only)          */
-    FE_FIELD_COUNT = 14
+    FE_FIELD_IMAGE = 14,        /* float4[height][width] RGBA of the last
+                                   fe_raymarch (download only)               */
+    FE_FIELD_COUNT = 15
 } fe_field;
 
 /* Step flags for fe_step. */
@@ -320,6 +322,26 @@ FE_API fe_status fe_stats_pass(fe_ctx* ctx);
  * fe_download(FE_FIELD_DENSITY_GRID).  Enqueued on the context's stream;
  * single-scene contexts only; grid_res in 1..1024 per axis. */
 FE_API fe_status fe_density_splat(fe_ctx* ctx);
+
+/* The water pass (water_pipeline.rs, entities/water.rs:136-152,
+ * raymarch.vert/.frag) without a graphics API: one ray per pixel through the
+ * last fe_density_splat grid, into the context's RGBA32F image (read with
+ * fe_download(FE_FIELD_IMAGE)).  Pixels the shader discards get alpha 0.
+ * The box is params.box_min/box_max (the water model's bounds); the sky is an
+ * equirectangular RGBA32F image [height][width] (row 0 at v = 0), sampled
+ * bilinearly with clamp-to-edge like the skybox sampler (water.rs:78-84).
+ * inv_view_proj is column-major (GLSL mat4 layout) and maps Vulkan NDC
+ * (y down, depth 0..1) to world space; a pixel's ray runs from camera_pos
+ * through the far-plane point of its centre. */
+typedef struct fe_camera {
+    float inv_view_proj[16];
+    float camera_pos[3];
+    uint32_t width;
+    uint32_t height;
+    uint32_t reserved[3];
+} fe_camera;
+FE_API fe_status fe_set_skybox(fe_ctx* ctx, const float* rgba, uint32_t width, uint32_t height);
+FE_API fe_status fe_raymarch(fe_ctx* ctx, const fe_camera* camera);
 
 /* Reads the stats of the last stats pass (host read of `stats_buffer`,
  * renderer/mod.rs:231-236).  Synchronises the context's stream. */

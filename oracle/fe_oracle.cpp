@@ -1024,6 +1024,163 @@ void fo_splat_density(const float* pos4, uint32_t n, const fe_params* p, uint32_
     }
 }
 
+// raymarch.frag:1-215, restated for one ray per pixel (see fo_raymarch in
+// fe_oracle.h for the conventions).  Transcendentals are the host's libm.
+namespace rm {
+struct V {
+    float x, y, z;
+};
+inline V v(float x, float y, float z) { return {x, y, z}; }
+inline V add(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V sub(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V mul(V a, V b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline V muls(V a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V divv(V a, V b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
+inline float dot(V a, V b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V normalize(V a) {
+    float l = std::sqrt(dot(a, a));
+    return {a.x / l, a.y / l, a.z / l};
+}
+inline float mix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+inline V mixv(V a, V b, float t) { return {mix(a.x, b.x, t), mix(a.y, b.y, t), mix(a.z, b.z, t)}; }
+inline float clampf(float x, float lo, float hi) { return std::fmin(std::fmax(x, lo), hi); }
+inline float smoothstep(float e0, float e1, float x) {
+    float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+struct Grid {
+    const uint32_t* g;
+    int rx, ry, rz;
+    V bmin, bmax;
+    float fetch(int x, int y, int z) const {
+        x = std::min(std::max(x, 0), rx - 1);
+        y = std::min(std::max(y, 0), ry - 1);
+        z = std::min(std::max(z, 0), rz - 1);
+        return (float)g[((size_t)z * ry + y) * rx + x];
+    }
+    float density(V p) const {  // getDensity
+        V uvw = divv(sub(p, bmin), sub(bmax, bmin));
+        if (uvw.x < 0.0f || uvw.y < 0.0f || uvw.z < 0.0f || uvw.x > 1.0f || uvw.y > 1.0f ||
+            uvw.z > 1.0f)
+            return 0.0f;
+        float gx = uvw.x * (float)rx - 0.5f, gy = uvw.y * (float)ry - 0.5f,
+              gz = uvw.z * (float)rz - 0.5f;
+        float fx = std::floor(gx), fy = std::floor(gy), fz = std::floor(gz);
+        int ix = to_int_sat<float>(fx), iy = to_int_sat<float>(fy), iz = to_int_sat<float>(fz);
+        float tx = gx - fx, ty = gy - fy, tz = gz - fz;
+        float v0 = mix(mix(fetch(ix, iy, iz), fetch(ix + 1, iy, iz), tx),
+                       mix(fetch(ix, iy + 1, iz), fetch(ix + 1, iy + 1, iz), tx), ty);
+        float v1 = mix(mix(fetch(ix, iy, iz + 1), fetch(ix + 1, iy, iz + 1), tx),
+                       mix(fetch(ix, iy + 1, iz + 1), fetch(ix + 1, iy + 1, iz + 1), tx), ty);
+        return std::fmax(0.0f, (mix(v0, v1, tz) - 300.0f) * 1.0f);
+    }
+};
+inline V sky(const float* s, int w, int h, V dir) {  // sampleSkybox, bilinear clamp-to-edge
+    dir = normalize(dir);
+    float u = std::atan2(dir.z, dir.x) * 0.15915f + 0.5f;
+    float vv = std::asin(clampf(dir.y, -1.0f, 1.0f)) * 0.31831f + 0.5f;
+    float x = u * (float)w - 0.5f, y = vv * (float)h - 0.5f;
+    float x0f = std::floor(x), y0f = std::floor(y);
+    float ax = x - x0f, ay = y - y0f;
+    int x0 = to_int_sat<float>(x0f), y0 = to_int_sat<float>(y0f);
+    auto at = [&](int xi, int yi) {
+        xi = std::min(std::max(xi, 0), w - 1);
+        yi = std::min(std::max(yi, 0), h - 1);
+        const float* c = s + 4 * ((size_t)yi * w + xi);
+        return v(c[0], c[1], c[2]);
+    };
+    V c0 = mixv(at(x0, y0), at(x0 + 1, y0), ax), c1 = mixv(at(x0, y0 + 1), at(x0 + 1, y0 + 1), ax);
+    return mixv(c0, c1, ay);
+}
+}  // namespace rm
+
+void fo_raymarch(const uint32_t* grid, int rx, int ry, int rz, const float* sky4, int sky_w,
+                 int sky_h, const float* inv_view_proj, const float* cam_pos,
+                 const float* box_min, const float* box_max, int width, int height, float* out) {
+    using namespace rm;
+    const float* M = inv_view_proj;
+    V size = v(box_max[0] - box_min[0], box_max[1] - box_min[1], box_max[2] - box_min[2]);
+    V center = v(box_min[0] + size.x * 0.5f, box_min[1] + size.y * 0.5f, box_min[2] + size.z * 0.5f);
+    V scale = v(std::sqrt(size.x * size.x), std::sqrt(size.y * size.y), std::sqrt(size.z * size.z));
+    Grid G{grid, rx, ry, rz, sub(center, muls(scale, 0.5f)), add(center, muls(scale, 0.5f))};
+    const V cam = v(cam_pos[0], cam_pos[1], cam_pos[2]);
+    const V L = normalize(v(0.4f, 1.0f, 0.3f));
+    const V sun = v(1.0f, 0.95f, 0.85f), scatter = v(0.04f, 0.18f, 0.28f);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads())
+    for (int py = 0; py < height; ++py)
+        for (int px = 0; px < width; ++px) {
+            float* o = out + 4 * ((size_t)py * width + px);
+            float nx = ((float)px + 0.5f) / (float)width * 2.0f - 1.0f;
+            float ny = ((float)py + 0.5f) / (float)height * 2.0f - 1.0f;
+            float w4[4];
+            for (int r = 0; r < 4; ++r) w4[r] = ((M[r] * nx + M[4 + r] * ny) + M[8 + r] * 1.0f) + M[12 + r] * 1.0f;
+            V rd = normalize(sub(v(w4[0] / w4[3], w4[1] / w4[3], w4[2] / w4[3]), cam));
+            V t1 = divv(sub(G.bmin, cam), rd), t2 = divv(sub(G.bmax, cam), rd);
+            float tn = std::fmax(std::fmax(std::fmin(t1.x, t2.x), std::fmin(t1.y, t2.y)), std::fmin(t1.z, t2.z));
+            float tf = std::fmin(std::fmin(std::fmax(t1.x, t2.x), std::fmax(t1.y, t2.y)), std::fmax(t1.z, t2.z));
+            o[0] = o[1] = o[2] = o[3] = 0.0f;
+            if (tn > tf || tf < 0.0f) continue;
+            float step = 0.007f * std::fmax(std::fmax(scale.x, scale.y), scale.z);
+            float tc = std::fmax(tn, 0.0f);
+            bool hit = false;
+            for (int i = 0; i < 96; i++) {
+                if (tc > tf) break;
+                if (G.density(add(cam, muls(rd, tc))) > 0.01f) {
+                    hit = true;
+                    break;
+                }
+                tc += step;
+            }
+            if (!hit) continue;
+            float ta = tc - step, tb = tc;
+            for (int i = 0; i < 8; i++) {
+                float m = (ta + tb) * 0.5f;
+                if (G.density(add(cam, muls(rd, m))) > 0.01f) tb = m;
+                else ta = m;
+            }
+            V sp = add(cam, muls(rd, tb));
+            const float e = 0.018f;
+            V n = normalize(v(G.density(add(sp, v(e, 0, 0))) - G.density(sub(sp, v(e, 0, 0))),
+                              G.density(add(sp, v(0, e, 0))) - G.density(sub(sp, v(0, e, 0))),
+                              G.density(add(sp, v(0, 0, e))) - G.density(sub(sp, v(0, 0, e)))));
+            V N = normalize(v(-n.x, -n.y, -n.z));
+            if (dot(N, N) < 0.5f) N = v(0.0f, 1.0f, 0.0f);
+            V Vw = v(-rd.x, -rd.y, -rd.z);
+            V H = normalize(add(L, Vw));
+            float ndv = std::fmax(dot(N, Vw), 0.0f), ndl = std::fmax(dot(N, L), 0.0f),
+                  ndh = std::fmax(dot(N, H), 0.0f);
+            float f0 = std::pow((1.0f - 1.333f) / (1.0f + 1.333f), 2.0f);
+            float F = clampf(f0 + (1.0f - f0) * std::pow(clampf(1.0f - ndv, 0.0f, 1.0f), 5.0f), 0.0f, 1.0f);
+            V refl = sub(rd, muls(N, 2.0f * dot(N, rd)));
+            V reflection = sky(sky4, sky_w, sky_h, refl);
+            float a = 0.04f * 0.04f, a2 = a * a, dd = ndh * ndh * (a2 - 1.0f) + 1.0f;
+            float spec = a2 / (3.14159f * dd * dd) * ndl;
+            reflection = add(reflection, muls(sun, clampf(spec * 0.15f, 0.0f, 3.0f)));
+            float thickness = 0.0f, t = 0.0f, tmax = tf - tb;
+            for (int i = 0; i < 64 && t < tmax; i++, t += 0.015f)
+                if (G.density(add(sp, muls(rd, t))) > 0.01f) thickness += 0.015f;
+            V absorption = v(std::exp(-0.45f * thickness * 8.0f), std::exp(-0.085f * thickness * 8.0f),
+                             std::exp(-0.025f * thickness * 8.0f));
+            float eta = 1.0f / 1.333f, ni = dot(N, rd), k = 1.0f - eta * eta * (1.0f - ni * ni);
+            V refr = k < 0.0f ? v(0, 0, 0) : sub(muls(rd, eta), muls(N, eta * ni + std::sqrt(k)));
+            if (dot(refr, refr) < 0.01f) refr = rd;
+            V background = sky(sky4, sky_w, sky_h, normalize(refr));
+            float sw = std::fmax(0.0f, dot(N, L) * 0.5f + 0.5f);
+            float sb = std::fmax(0.0f, dot(v(-N.x, -N.y, -N.z), L));
+            float sf = (sw * 0.6f + sb * 0.4f) * (1.0f - std::exp(-thickness * 3.0f));
+            V sss = muls(muls(mul(scatter, sun), sf), 0.35f);
+            float foam = smoothstep(0.0f, 0.3f, thickness) * smoothstep(0.5f, 0.95f, N.y);
+            V refracted = add(mul(background, absorption), sss);
+            V water = mixv(refracted, reflection, F);
+            water = mixv(water, muls(v(0.92f, 0.96f, 1.0f), ndl * 0.7f + 0.3f), foam * 0.7f);
+            water = add(water, muls(scatter, 0.04f));
+            o[0] = water.x / (water.x + 1.0f);
+            o[1] = water.y / (water.y + 1.0f);
+            o[2] = water.z / (water.z + 1.0f);
+            o[3] = 1.0f;
+        }
+}
+
 int fo_set_threads(int t) {
     g_threads = t;
     return nthreads();

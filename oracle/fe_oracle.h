@@ -82,6 +82,15 @@ double fo_det_sum(const double* values, size_t n);
  * out[grid_res z][y][x] (cleared first). */
 void fo_splat_density(const float* pos4, uint32_t n, const fe_params* params, uint32_t* out);
 
+/* raymarch.frag:1-215 for one ray per pixel: the ray from cam_pos through
+ * the far-plane point of the pixel centre under the column-major
+ * inv_view_proj (Vulkan NDC); grid[rz][ry][rx] the splat; sky4[h][w] RGBA,
+ * bilinear clamp-to-edge; out[height][width] RGBA, alpha 0 where the shader
+ * discards. */
+void fo_raymarch(const uint32_t* grid, int rx, int ry, int rz, const float* sky4, int sky_w,
+                 int sky_h, const float* inv_view_proj, const float* cam_pos,
+                 const float* box_min, const float* box_max, int width, int height, float* out);
+
 int fo_set_threads(int threads);
 int fo_get_threads(void);
 

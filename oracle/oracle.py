@@ -53,6 +53,9 @@ def lib():
             "fo_sort_bitonic": (c_int, [c_void_p, c_void_p, c_uint32]),
             "fo_det_sum": (c_double, [c_void_p, c_size_t]),
             "fo_splat_density": (None, [c_void_p, c_uint32, P, c_void_p]),
+            "fo_raymarch": (None, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
+                                   c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                   c_void_p]),
             "fo_set_threads": (c_int, [c_int]),
             "fo_get_threads": (c_int, []),
         }
@@ -182,6 +185,22 @@ def splat_density(positions4, params) -> np.ndarray:
     out = np.empty((rz, ry, rx), dtype=np.uint32)
     p = _abi.copy_params(params)
     lib().fo_splat_density(_ptr(pos), pos.shape[0], ctypes.byref(p), _ptr(out))
+    return out
+
+
+def raymarch(grid, sky, camera, box_min, box_max) -> np.ndarray:
+    """raymarch.frag for one ray per pixel: float32[height][width][4]."""
+    g = np.ascontiguousarray(grid, dtype=np.uint32)
+    rz, ry, rx = g.shape
+    sk = np.ascontiguousarray(sky, dtype=np.float32)
+    sh, sw = sk.shape[:2]
+    ivp = np.ascontiguousarray(np.frombuffer(bytes(camera.inv_view_proj), np.float32))
+    cam = np.ascontiguousarray(np.frombuffer(bytes(camera.camera_pos), np.float32))
+    bmin = np.ascontiguousarray(box_min, np.float32)
+    bmax = np.ascontiguousarray(box_max, np.float32)
+    out = np.empty((camera.height, camera.width, 4), np.float32)
+    lib().fo_raymarch(_ptr(g), rx, ry, rz, _ptr(sk), sw, sh, _ptr(ivp), _ptr(cam), _ptr(bmin),
+                      _ptr(bmax), camera.width, camera.height, _ptr(out))
     return out
 
 
