@@ -281,6 +281,8 @@ struct fe_ctx {
     int splat_res[3] = {0, 0, 0};  // resolution of the last splat
     int4* splat_taps = nullptr;
     uint32_t splat_ntaps = 0;
+    uint32_t* splat_hist = nullptr;    // particles per centre voxel
+    size_t splat_hist_cap = 0;
 
     // raymarched image and its sky
     float4* sky = nullptr;
@@ -1195,12 +1197,22 @@ fe_status fe_density_splat(fe_ctx* c) {
     c->splat_res[0] = rx;
     c->splat_res[1] = ry;
     c->splat_res[2] = rz;
+    // Counts per centre voxel, then the convolution with the tap table
+    // (fe_splat.cu).
+    const int3 res = make_int3(rx, ry, rz);
+    const size_t hist_n = (size_t)(rx + 1) * (ry + 1) * (rz + 1);
+    if (hist_n > c->splat_hist_cap) {
+        fe_status st0 = dev_alloc(c, &c->splat_hist, hist_n);
+        if (st0 != FE_OK) return st0;
+        c->splat_hist_cap = hist_n;
+    }
+    const float3 b0 = make_float3(p.box_min[0], p.box_min[1], p.box_min[2]);
+    const float3 b1 = make_float3(p.box_max[0], p.box_max[1], p.box_max[2]);
     FE_CUDA(cudaMemsetAsync(c->splat_grid, 0, voxels * 4, c->stream));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    FE_CUDA(splat(c->B.pos_a, c->n, make_float3(p.box_min[0], p.box_min[1], p.box_min[2]),
-                  make_float3(p.box_max[0], p.box_max[1], p.box_max[2]), make_int3(rx, ry, rz),
-                  c->splat_taps, c->splat_ntaps, c->splat_grid, c->stream, sms));
+    FE_CUDA(cudaMemsetAsync(c->splat_hist, 0, hist_n * 4, c->stream));
+    FE_CUDA(splat_histogram(c->B.pos_a, c->n, b0, b1, res, c->splat_hist, c->stream));
+    FE_CUDA(splat_convolve(c->splat_hist, res, c->splat_taps, c->splat_ntaps, c->splat_grid,
+                           c->stream));
     return FE_OK;
 }
 
