@@ -193,14 +193,16 @@ def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = Fal
     """Kernels of one frame with one substep (the frame graph's nodes)."""
     # neighbour search: hash, scratch fill, histogram, P passes, table fill,
     # offsets, reorder (+ pressure carry in FIXED mode, + learned state)
-    ns = 1 + 1 + 1 + passes + 1 + 1 + 1 + (1 if fixed_mode else 0) + (2 if learned else 0)
+    ns = 1 + 1 + 1 + passes + 1 + 1 + 1 + (1 if fixed_mode else 0) + \
+        (1 if learned and not fixed_mode else 0)
     # viscosity, density source, 2 x (solve begin + end), integration, density/alpha,
     # divergence source, divergence integration, substep counter
     fixed = 1 + 1 + 4 + 1 + 1 + 1 + 1 + 1
     # per Jacobi iteration: force, update, loop guard
     iters = 3 * (stats.density_iterations + stats.divergence_iterations)
-    # learned: 2 x (features, network, apply, after-solve)
-    extra = 8 if learned else 0
+    # learned: 2 x (network, apply); features, after-solve bookkeeping and the
+    # carry permutation ride in the source, integration and reorder passes
+    extra = 4 if learned else 0
     return 1 + ns + fixed + iters + extra + 1   # + prologue, stats
 
 

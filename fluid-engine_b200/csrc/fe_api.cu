@@ -378,11 +378,17 @@ fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
     REC(R.k(k_fill_cells, dim3(std::min<uint32_t>((c->T + 255) / 256, 148 * 8)), dim3(256),
             B.cells, (size_t)c->T));
     REC(R.k(k_offsets, flat_grid(c->n), dim3(kBlock), B));
-    REC(R.k(k_reorder, flat_grid(c->n), dim3(kBlock), B, c->fixed_mode() ? 1 : 0));
-    if (c->fixed_mode()) REC(R.k(k_take_pressure, flat_grid(c->n), dim3(kBlock), B));
+    const int fixed = c->fixed_mode() ? 1 : 0;
     if (c->carries()) {
-        REC(R.k(k_carry_gather, flat_grid(c->n), dim3(kBlock), B, c->L));
-        REC(R.k(k_carry_take, flat_grid(c->n), dim3(kBlock), B, c->L));
+        // the learned state rides along with the gather and the copy-back
+        REC(R.k(k_reorder_carry, flat_grid(c->n), dim3(kBlock), B, fixed, c->L));
+        if (fixed)
+            REC(R.k(k_take_pressure_carry, flat_grid(c->n), dim3(kBlock), B, c->L));
+        else
+            REC(R.k(k_carry_take, flat_grid(c->n), dim3(kBlock), B, c->L));
+    } else {
+        REC(R.k(k_reorder, flat_grid(c->n), dim3(kBlock), B, fixed));
+        if (fixed) REC(R.k(k_take_pressure, flat_grid(c->n), dim3(kBlock), B));
     }
     return FE_OK;
 }
@@ -472,8 +478,10 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 0));
     }
     if ((s = rec_solve(c, R, 0))) return s;
-    if (c->carries()) REC(R.k(k_after_solve, chunk_grid(c), dim3(kBlock), B, c->L, 0));
-    if ((s = rec_simple(c, R, k_pressure_integration))) return s;
+    if (c->carries())
+        REC(R.k(k_pressure_integration_learn, chunk_grid(c), dim3(kBlock), B, c->L));
+    else if ((s = rec_simple(c, R, k_pressure_integration)))
+        return s;
     if ((s = rec_neighbor_search(c, R))) return s;
     if ((s = rec_simple(c, R, k_density_alpha))) return s;
     if (c->carries())
@@ -485,8 +493,10 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 1));
     }
     if ((s = rec_solve(c, R, 1))) return s;
-    if (c->carries()) REC(R.k(k_after_solve, chunk_grid(c), dim3(kBlock), B, c->L, 1));
-    REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), B, fixed));
+    if (c->carries())
+        REC(R.k(k_divergence_integration_learn, chunk_grid(c), dim3(kBlock), B, fixed, c->L));
+    else
+        REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), B, fixed));
     REC(R.k(k_count_substep, dim3((B.n_scenes + 63) / 64), dim3(64), B));
     return FE_OK;
 }
@@ -644,6 +654,8 @@ fe_status collect_stats(fe_ctx* c, fe_stats* out, uint32_t scene = 0) {
     out->avg_divergence_error_f64 = S.stats_f64[1];
     out->density_residual = S.last_metric[0];
     out->divergence_residual = S.last_metric[1];
+    out->density_residual_max = S.last_metric_max[0];
+    out->divergence_residual_max = S.last_metric_max[1];
     out->density_iterations = S.last_iters[0];
     out->divergence_iterations = S.last_iters[1];
     out->total_density_iterations = S.total_iters[0];

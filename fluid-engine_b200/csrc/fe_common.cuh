@@ -126,6 +126,23 @@ __device__ __forceinline__ double block_tree256(double v, double* smem) {
     return r;
 }
 
+// Maximum of one value per thread of a 256-thread block (order-free).
+// Result valid in thread 0.
+__device__ __forceinline__ double block_max256(double v, double* smem) {
+    for (int m = 16; m >= 1; m >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, m));
+    const int warp = threadIdx.x >> 5;
+    if (lane_id() == 0) smem[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0) {
+        double w = lane_id() < 8 ? smem[lane_id()] : 0.0;
+        for (int m = 4; m >= 1; m >>= 1) w = fmax(w, __shfl_xor_sync(kFull, w, m));
+        r = w;
+    }
+    __syncthreads();
+    return r;
+}
+
 // Final stage of the fixed-order sum over `chunks` partials: thread t adds
 // partials t, t+256, ... in order, then block_tree256.  Valid in thread 0.
 __device__ __forceinline__ double block_final_sum(const double* partials, uint32_t chunks,

@@ -44,6 +44,7 @@ struct SolveCtl {
     uint32_t done;     // scene finished this solve
     uint32_t cap_hit;  // tolerance solve stopped at max_it
     double metric;     // tolerance metric of the last iteration
+    double metric_max; // largest per-particle error of the last iteration (same units)
 };
 
 struct SceneState {
@@ -54,6 +55,7 @@ struct SceneState {
     SolveCtl solve[2];
     uint32_t last_iters[2];
     double last_metric[2];
+    double last_metric_max[2];
     unsigned long long total_iters[2];
     uint32_t cap_hits;
     uint32_t substeps;

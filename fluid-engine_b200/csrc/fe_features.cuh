@@ -119,4 +119,26 @@ __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
     L.carry[i].w = __uint_as_float(slot);
 }
 
+// After solve `which`: the final pressure becomes the particle's "last kappa"
+// and, in capture mode, the training target of its sample slot (for the
+// divergence solve relative to the substep's density kappa, as the warm start
+// applies it).  Fused into the integration pass that follows each solve.
+__device__ __forceinline__ void after_solve_particle(const Bufs& B, const LearnArgs& L,
+                                                     const DevParams& P, uint32_t i, int which) {
+    const float p = B.prs[i];
+    float4 cr = L.carry[i];
+    const float base = which == 1 ? cr.x : 0.0f;
+    if (which == 0)
+        cr.x = p;
+    else
+        cr.y = p;
+    const uint32_t slot = __float_as_uint(cr.w);
+    if (L.capture && slot != 0xFFFFFFFFu && slot < L.cap_capacity) {
+        const float scale = kappa_scale(B.rho[i], B.alpha[i], P.dt, P.rho0);
+        L.cap_y[2 * (size_t)slot + which] = scale > 0.0f ? (p - base) / scale : 0.0f;
+    }
+    cr.w = __uint_as_float(0xFFFFFFFFu);
+    L.carry[i] = cr;
+}
+
 }  // namespace fe

@@ -65,7 +65,10 @@ __global__ void k_offsets(Bufs B) {
 // reorder.comp:37-46.  FIXED mode also gathers the pressures into prs_tmp.
 // The neighbour list of the old order is invalidated: until density_alpha
 // rebuilds it, the neighbour passes walk the new buckets.
-__global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) {
+// kCarry: the learned warm start's per-particle state is gathered too.
+template <bool kCarry>
+__device__ __forceinline__ void reorder_body(const Bufs& B, int carry_pressure,
+                                             const LearnArgs& L) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
     uint32_t src = B.vals[i];
@@ -79,16 +82,35 @@ __global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) 
     *rec_pos(B, i) = p;
     B.vel_b[i] = __ldg(B.vel_a + src);
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
+    if (kCarry) L.carry_tmp[i] = L.carry[src];
+}
+
+__global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) {
+    reorder_body<false>(B, carry_pressure, LearnArgs{});
+}
+__global__ void __launch_bounds__(kBlock) k_reorder_carry(Bufs B, int carry_pressure,
+                                                          LearnArgs L) {
+    reorder_body<true>(B, carry_pressure, L);
 }
 
 // FIXED mode: the gathered pressures become current; pr = p / rho^2 keeps
-// matching the (not yet recomputed) densities.
-__global__ void __launch_bounds__(kBlock) k_take_pressure(Bufs B) {
+// matching the (not yet recomputed) densities.  kCarry: the gathered learned
+// state too.
+template <bool kCarry>
+__device__ __forceinline__ void take_pressure_body(const Bufs& B, const LearnArgs& L) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
     float p = B.prs_tmp[i];
     B.prs[i] = p;
     posb(B, i)->w = pressure_over_rho2(p, B.rho[i]);
+    if (kCarry) L.carry[i] = L.carry_tmp[i];
+}
+
+__global__ void __launch_bounds__(kBlock) k_take_pressure(Bufs B) {
+    take_pressure_body<false>(B, LearnArgs{});
+}
+__global__ void __launch_bounds__(kBlock) k_take_pressure_carry(Bufs B, LearnArgs L) {
+    take_pressure_body<true>(B, L);
 }
 
 // pr = p / rho^2 for all particles (after a host upload of p or rho).
@@ -331,16 +353,23 @@ __device__ void solve_finish(Bufs& B, int which, cudaGraphConditionalHandle hand
         SolveCtl& ctl = B.S[s].solve[which];
         uint32_t nchunks = (P.n + kBlock - 1) / kBlock;
         bool active = !ctl.done;
-        double sum = 0.0;
-        if (active && P.solver == 1u)
+        double sum = 0.0, mx = 0.0;
+        if (active && P.solver == 1u) {
             sum = block_final_sum(B.partials + c0, nchunks, smem);
+            double m = 0.0;
+            for (uint32_t k = threadIdx.x; k < nchunks; k += kBlock)
+                m = fmax(m, __ldcg(B.partials + B.n_chunks + c0 + k));
+            mx = block_max256(m, smem);
+        }
         if (threadIdx.x == 0 && active) {
             ctl.iter += 1;
             if (P.solver == 1u) {
                 double avg = sum / (double)P.n;
                 if (which == 1) avg = avg * (double)P.dt;
                 double metric = avg / (double)P.rho0;
+                double metric_max = (which == 1 ? mx * (double)P.dt : mx) / (double)P.rho0;
                 ctl.metric = metric;
+                ctl.metric_max = metric_max;
                 float tol = which == 0 ? P.tol_d : P.tol_v;
                 if (ctl.iter >= P.min_it && metric <= (double)tol) {
                     ctl.done = 1;
@@ -404,10 +433,15 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
         }
     }
     if (!control) return;
-    // Per-chunk partial of the fixed-order sum (uniform branch per block).
+    // Per-chunk partial of the fixed-order sum and the chunk's largest error
+    // (uniform branch per block).
     if (!skip && P.solver == 1u) {
         double part = block_tree256(e_sum_in, smem);
-        if (threadIdx.x == 0) B.partials[c] = part;
+        double mx = block_max256(e_sum_in, smem);
+        if (threadIdx.x == 0) {
+            B.partials[c] = part;
+            B.partials[B.n_chunks + c] = mx;
+        }
     }
     if (last_block_done(&B.G->tickets[kTicketSolve], gridDim.x)) {
         solve_finish(B, which, handle, use_handle, smem);
@@ -430,6 +464,7 @@ __global__ void k_solve_begin(Bufs B, int which, cudaGraphConditionalHandle hand
         ctl.iter = 0;
         ctl.cap_hit = 0;
         ctl.metric = 0.0;
+        ctl.metric_max = 0.0;
         ctl.K = which == 0 ? B.S[s].iters_rho : B.S[s].iters_div;
         ctl.done = (P.solver == 1u) ? (P.max_it == 0u) : (ctl.K == 0u);
         if (!ctl.done) any_open = 1;
@@ -461,6 +496,7 @@ __global__ void k_solve_end(Bufs B, int which) {
         SolveCtl& ctl = S.solve[which];
         S.last_iters[which] = ctl.iter;
         S.last_metric[which] = ctl.metric;
+        S.last_metric_max[which] = ctl.metric_max;
         S.total_iters[which] += ctl.iter;
         if (ctl.cap_hit) {
             S.cap_hits += 1;
@@ -473,7 +509,8 @@ __global__ void k_solve_end(Bufs B, int which) {
 // pressure_integration.comp:16-77: position_b in, position_a and velocity_a
 // out.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_pressure_integration(Bufs B) {
+template <bool kLearn>
+__device__ __forceinline__ void pressure_integration_body(const Bufs& B, const LearnArgs& L) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
@@ -501,16 +538,36 @@ __global__ void __launch_bounds__(kBlock) k_pressure_integration(Bufs B) {
     }
     B.pos_a[i] = make_float4(np.x, np.y, np.z, 1.0f);
     B.vel_a[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+    if (kLearn) after_solve_particle(B, L, P, i, 0);
+}
+
+__global__ void __launch_bounds__(kBlock) k_pressure_integration(Bufs B) {
+    pressure_integration_body<false>(B, LearnArgs{});
+}
+// + the density solve's after-solve bookkeeping of the learned warm start
+__global__ void __launch_bounds__(kBlock) k_pressure_integration_learn(Bufs B, LearnArgs L) {
+    pressure_integration_body<true>(B, L);
 }
 
 // divergence_integration.comp:14-43 (velocity; colour is render-only).
-__global__ void __launch_bounds__(kBlock) k_divergence_integration(Bufs B, int fixed) {
+template <bool kLearn>
+__device__ __forceinline__ void divergence_integration_body(const Bufs& B, int fixed,
+                                                            const LearnArgs& L) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     float4* vel = fixed ? B.vel_b : B.vel_a;
     f3 nv = add(xyz(vel[i]), scale_r(xyz(*accp(B, i)), P.dt));
     vel[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+    if (kLearn) after_solve_particle(B, L, P, i, 1);
+}
+
+__global__ void __launch_bounds__(kBlock) k_divergence_integration(Bufs B, int fixed) {
+    divergence_integration_body<false>(B, fixed, LearnArgs{});
+}
+__global__ void __launch_bounds__(kBlock) k_divergence_integration_learn(Bufs B, int fixed,
+                                                                          LearnArgs L) {
+    divergence_integration_body<true>(B, fixed, L);
 }
 
 // ---------------------------------------------------------------------------

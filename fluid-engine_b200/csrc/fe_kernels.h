@@ -14,7 +14,9 @@ __global__ void k_fill_cells(uint2* p, size_t count);
 __global__ void k_hash(Bufs B);
 __global__ void k_offsets(Bufs B);
 __global__ void k_reorder(Bufs B, int carry_pressure);
+__global__ void k_reorder_carry(Bufs B, int carry_pressure, LearnArgs L);
 __global__ void k_take_pressure(Bufs B);
+__global__ void k_take_pressure_carry(Bufs B, LearnArgs L);
 __global__ void k_refresh_pr(Bufs B);
 __global__ void k_density_alpha(Bufs B);
 __global__ void k_viscosity(Bufs B);
@@ -28,15 +30,15 @@ __global__ void k_solve_begin(Bufs B, int which, cudaGraphConditionalHandle hand
 __global__ void k_solve_end(Bufs B, int which);
 __global__ void k_loop_guard(Bufs B, int which, cudaGraphConditionalHandle handle);
 __global__ void k_pressure_integration(Bufs B);
+__global__ void k_pressure_integration_learn(Bufs B, LearnArgs L);
 __global__ void k_divergence_integration(Bufs B, int fixed);
+__global__ void k_divergence_integration_learn(Bufs B, int fixed, LearnArgs L);
 __global__ void k_stats(Bufs B, int fixed, uint4* upart);
 __global__ void k_frame_prologue(Bufs B);
 __global__ void k_count_substep(Bufs B);
 __global__ void k_density_source_learn(Bufs B, LearnArgs L);
 __global__ void k_divergence_source_learn(Bufs B, int fixed, LearnArgs L);
 __global__ void k_warm_apply(Bufs B, LearnArgs L, int which);
-__global__ void k_after_solve(Bufs B, LearnArgs L, int which);
-__global__ void k_carry_gather(Bufs B, LearnArgs L);
 __global__ void k_carry_take(Bufs B, LearnArgs L);
 
 }  // namespace fe

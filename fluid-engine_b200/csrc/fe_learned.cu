@@ -4,9 +4,10 @@
 // Before each of the two solves of a substep the source-term pass emits the
 // features (fe_features.cuh), the network (fe_mlp.cu) maps them to the
 // solve's initial pressure (output 0 for the density solve, output 1 for the
-// divergence solve) and k_warm_apply installs it.  After each solve the final pressure is recorded as the "last
-// kappa" feature and, in capture mode, as the target of the captured
-// particles (the other output's target is NaN: not trained).
+// divergence solve) and k_warm_apply installs it.  After each solve the
+// integration pass records the final pressure as the "last kappa" feature
+// and, in capture mode, as the target of the captured particles
+// (after_solve_particle; the other output's target is NaN: not trained).
 //
 // Feature definitions and normalisation: fe_features.cuh.
 #include <cuda_bf16.h>
@@ -38,6 +39,14 @@ namespace fe {
 // above 1, feeds such errors back from substep to substep and is not stable
 // either.  Under the bound the start stays near or below the solution,
 // where Jacobi approaches from the same side as the plain solver.
+//
+// Particles with fewer than kMinNeighbours neighbours (the free surface and
+// splashes, where alpha is small, scale_i large and training samples few)
+// keep the plain start.  Without this, a long adaptive-CFL run of the 262k
+// dam break still threw single particles out at 10^2 - 10^3 m/s late in the
+// run (a few over-pressured particles do not move the mean tolerance); with
+// it the largest speed matches the plain solver's.
+constexpr uint32_t kMinNeighbours = 16;
 __global__ void __launch_bounds__(kBlock) k_warm_apply(Bufs B, LearnArgs L, int which) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
@@ -53,46 +62,15 @@ __global__ void __launch_bounds__(kBlock) k_warm_apply(Bufs B, LearnArgs L, int 
         if (fabsf(a_ii) > 1e-20f) p1 = fmaxf((P.omega * B.src[i]) / a_ii, 0.0f);
     }
     const float d = p1 / P.omega;
-    float p = base + y * scale;
+    float p = B.nbr_count[i] < kMinNeighbours ? base : base + y * scale;
     p = p > 0.0f ? p : 0.0f;  // NaN -> 0; pressures are clamped at 0 as in pressure_update
     p = fminf(p, fmaxf(d, carry.x));
     B.prs[i] = p;
     posb(B, i)->w = pressure_over_rho2(p, rho);
 }
 
-// After a solve: the final pressure becomes the "last kappa" feature and, in
-// capture mode, the training target of the particle's slot (for the
-// divergence solve, relative to the density kappa as in k_warm_apply).
-__global__ void __launch_bounds__(kBlock) k_after_solve(Bufs B, LearnArgs L, int which) {
-    uint32_t i, s, c;
-    if (!chunk_of(B, i, s, c)) return;
-    const DevParams& P = B.P[s];
-    const float p = B.prs[i];
-    float4 cr = L.carry[i];
-    const float base = which == 1 ? cr.x : 0.0f;
-    if (which == 0)
-        cr.x = p;
-    else
-        cr.y = p;
-    const uint32_t slot = __float_as_uint(cr.w);
-    if (L.capture && slot != 0xFFFFFFFFu && slot < L.cap_capacity) {
-        const float scale = kappa_scale(B.rho[i], B.alpha[i], P.dt, P.rho0);
-        L.cap_y[2 * (size_t)slot + which] = scale > 0.0f ? (p - base) / scale : 0.0f;
-    }
-    cr.w = __uint_as_float(0xFFFFFFFFu);
-    L.carry[i] = cr;
-}
-
-// Carries the per-particle learned state through the re-sort: gather by the
-// sorted index, then copy back.
-__global__ void __launch_bounds__(kBlock) k_carry_gather(Bufs B, LearnArgs L) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n_total) return;
-    uint32_t src = B.vals[i];
-    if (src >= B.n_total) src = i;
-    L.carry_tmp[i] = L.carry[src];
-}
-
+// Copies the re-sorted learned state back (k_reorder_carry gathered it into
+// carry_tmp); FIXED mode does this inside k_take_pressure_carry.
 __global__ void __launch_bounds__(kBlock) k_carry_take(Bufs B, LearnArgs L) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;

@@ -385,8 +385,8 @@ struct TrainSmem {
     alignas(128) uint8_t doutT[2048 * 16];       // transposed, padded to 128 features
     alignas(128) uint8_t dz2T[2048 * 16];
     alignas(128) uint8_t dz1T[2048 * 16];
-    float db1[64], db2[64], db3[16];
-    float loss;
+    float db1[4][64], db2[4][64], db3[4][2];  // per warp: one writer each, summed in warp order
+    float loss[4];
     alignas(8) uint64_t bar;
     uint32_t tmem_base;
 };
@@ -396,10 +396,15 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// Each block writes its gradient sums (kParams floats in the Grads layout,
+// then the loss) to its own slice part[blockIdx.x][kParams + 1]; k_sum_parts
+// adds the slices in block order, so the result does not depend on timing.
 __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_bfloat16* __restrict__ X,
                                                           const float* __restrict__ Y, uint32_t n,
-                                                          float inv_count, Grads G,
+                                                          float inv_count, float* __restrict__ part,
                                                           uint32_t* error_flags) {
+    Grads G = grads_from(part + (size_t)blockIdx.x * (kParams + 1),
+                         part + (size_t)blockIdx.x * (kParams + 1) + kParams);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
     const uint32_t tid = threadIdx.x;
@@ -410,12 +415,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
         reinterpret_cast<uint4*>(S.dz2T)[t] = make_uint4(0, 0, 0, 0);
         reinterpret_cast<uint4*>(S.dz1T)[t] = make_uint4(0, 0, 0, 0);
     }
-    for (uint32_t t = tid; t < 64; t += kThreads) S.db1[t] = S.db2[t] = 0.0f;
-    if (tid < 16) S.db3[tid] = 0.0f;
-    if (tid == 0) {
-        S.loss = 0.0f;
-        bar_init(&S.bar);
-    }
+    for (uint32_t t = tid; t < 4 * 64; t += kThreads) (&S.db1[0][0])[t] = (&S.db2[0][0])[t] = 0.0f;
+    if (tid < 8) (&S.db3[0][0])[tid] = 0.0f;
+    if (tid < 4) S.loss[tid] = 0.0f;
+    if (tid == 0) bar_init(&S.bar);
     tmem_alloc(&S.tmem_base, 512);
     fence_async_smem();
     tc_before_sync();
@@ -498,9 +501,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
             float l = warp_sum(e0 * e0 + e1 * e1);
             float s0 = warp_sum(g0), s1 = warp_sum(g1);
             if ((tid & 31) == 0) {
-                atomicAdd(&S.loss, l);
-                atomicAdd(&S.db3[0], s0);
-                atomicAdd(&S.db3[1], s1);
+                S.loss[tid >> 5] += l;
+                S.db3[tid >> 5][0] += s0;
+                S.db3[tid >> 5][1] += s1;
             }
             for (int c = 0; c < 16; ++c) {
                 float gv = c == 0 ? g0 : (c == 1 ? g1 : 0.0f);
@@ -539,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
                     st_bf16(S.dz, off_k(row, c0 + i, 64), d);
                     st_bf16(S.dz2T, off_t(row, c0 + i), d);
                     float s = warp_sum(d);
-                    if ((tid & 31) == 0) atomicAdd(&S.db2[c0 + i], s);
+                    if ((tid & 31) == 0) S.db2[tid >> 5][c0 + i] += s;
                 }
             }
         }
@@ -573,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
                     float d = valid ? dh[i] * silu_grad(z[i] + S.W.b1[c0 + i]) : 0.0f;
                     st_bf16(S.dz1T, off_t(row, c0 + i), d);
                     float s = warp_sum(d);
-                    if ((tid & 31) == 0) atomicAdd(&S.db1[c0 + i], s);
+                    if ((tid & 31) == 0) S.db1[tid >> 5][c0 + i] += s;
                 }
             }
         }
@@ -595,7 +598,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
         tc_before_sync();
         __syncthreads();
     }
-    // ---- write the block's weight gradients (rows 0..63 / 0..15 of TMEM)
+    // ---- write the block's gradient sums to its slice (rows 0..63 / 0..15
+    // of TMEM for the weights; every element has one writer)
     if (ok && local_tiles > 0) {
         tc_after_sync();
         const uint32_t warp = tid >> 5;
@@ -603,26 +607,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_train(Params P, const __nv_
             float v[16];
             for (int c0 = 0; c0 < 64; c0 += 16) {
                 tmem_ld16(lane_addr(c_dw2, c0), v);
-                for (int i = 0; i < 16; ++i) atomicAdd(&G.w2[row * 64 + c0 + i], v[i]);
+                for (int i = 0; i < 16; ++i) G.w2[row * 64 + c0 + i] = v[i];
             }
             tmem_ld16(lane_addr(c_dw1, 0), v);
-            for (int i = 0; i < 16; ++i) atomicAdd(&G.w1[row * 16 + i], v[i]);
+            for (int i = 0; i < 16; ++i) G.w1[row * 16 + i] = v[i];
         }
         if (warp == 0) {
             float v[16];
             for (int c0 = 0; c0 < 64; c0 += 16) {
                 tmem_ld16(lane_addr(c_dw3, c0), v);
                 if (row < 2)
-                    for (int i = 0; i < 16; ++i) atomicAdd(&G.w3[row * 64 + c0 + i], v[i]);
+                    for (int i = 0; i < 16; ++i) G.w3[row * 64 + c0 + i] = v[i];
             }
         }
         __syncthreads();
         for (uint32_t t = tid; t < 64; t += kThreads) {
-            atomicAdd(&G.b1[t], S.db1[t]);
-            atomicAdd(&G.b2[t], S.db2[t]);
+            G.b1[t] = ((S.db1[0][t] + S.db1[1][t]) + S.db1[2][t]) + S.db1[3][t];
+            G.b2[t] = ((S.db2[0][t] + S.db2[1][t]) + S.db2[2][t]) + S.db2[3][t];
         }
-        if (tid < 2) atomicAdd(&G.b3[tid], S.db3[tid]);
-        if (tid == 0) atomicAdd(G.loss, S.loss);
+        if (tid < 2) G.b3[tid] = ((S.db3[0][tid] + S.db3[1][tid]) + S.db3[2][tid]) + S.db3[3][tid];
+        if (tid == 0) *G.loss = ((S.loss[0] + S.loss[1]) + S.loss[2]) + S.loss[3];
+    } else {
+        // no tile (or a timed-out wait): an all-zero slice
+        float* slice = part + (size_t)blockIdx.x * (kParams + 1);
+        for (uint32_t t = tid; t < kParams + 1; t += kThreads) slice[t] = 0.0f;
     }
     if (!ok && tid == 0) atomicOr(error_flags, 0x4u);
     tc_before_sync();
@@ -680,8 +688,20 @@ cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t 
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_sum_parts(const float* __restrict__ part, uint32_t blocks,
+                            float* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= kParams + 1) return;
+    float s = 0.0f;
+    for (uint32_t b = 0; b < blocks; ++b) s += part[(size_t)b * (kParams + 1) + t];
+    out[t] = s;
+}
+}  // namespace
+
 cudaError_t train_grads(const Params& P, const __nv_bfloat16* X, const float* Y, uint32_t n,
-                        const Grads& G, uint32_t* error_flags, cudaStream_t stream, int num_sms) {
+                        float* grad, float* part, uint32_t* error_flags, cudaStream_t stream,
+                        int num_sms) {
     if (n == 0) return cudaSuccess;
     static bool configured = false;
     size_t smem = train_smem_bytes();
@@ -693,7 +713,10 @@ cudaError_t train_grads(const Params& P, const __nv_bfloat16* X, const float* Y,
     }
     uint32_t tiles = (n + kTile - 1) / kTile;
     uint32_t grid = tiles < (uint32_t)num_sms ? tiles : (uint32_t)num_sms;
-    k_mlp_train<<<grid, kThreads, smem, stream>>>(P, X, Y, n, 1.0f / (float)n, G, error_flags);
+    k_mlp_train<<<grid, kThreads, smem, stream>>>(P, X, Y, n, 1.0f / (float)n, part, error_flags);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_sum_parts<<<(kParams + 1 + 255) / 256, 256, 0, stream>>>(part, grid, grad);
     return cudaGetLastError();
 }
 

@@ -29,11 +29,11 @@ struct Grads {
     float* loss;
 };
 
-inline Params params_from(const __nv_bfloat16* wbf16, const float* master) {
+__host__ __device__ inline Params params_from(const __nv_bfloat16* wbf16, const float* master) {
     return Params{wbf16, wbf16 + kW1, wbf16 + kW1 + kW2, master + kWeights,
                   master + kWeights + 64, master + kWeights + 128};
 }
-inline Grads grads_from(float* g, float* loss) {
+__host__ __device__ inline Grads grads_from(float* g, float* loss) {
     return Grads{g, g + kW1, g + kW1 + kW2, g + kWeights, g + kWeights + 64, g + kWeights + 128,
                  loss};
 }
@@ -62,10 +62,14 @@ cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t 
                   uint32_t* error_flags, cudaStream_t stream, int num_sms,
                   int ctas_per_sm = kInferDefaultCtasPerSm);
 
-// Adds d(loss)/d(params) of the mean squared error over the n samples to G
-// (G must be zeroed by the caller; Adam zeroes it after each step).
+// Writes d(loss)/d(params) of the mean squared error over the n samples to
+// grad[kParams] and the summed squared error to grad[kParams].  Blocks sum
+// their tiles into their own slice of part[min(tiles, num_sms)][kParams + 1],
+// and the slices are added in block order: the same inputs give the same
+// gradients bit for bit.
 cudaError_t train_grads(const Params& P, const __nv_bfloat16* X, const float* Y, uint32_t n,
-                        const Grads& G, uint32_t* error_flags, cudaStream_t stream, int num_sms);
+                        float* grad, float* part, uint32_t* error_flags, cudaStream_t stream,
+                        int num_sms);
 
 cudaError_t adam(float* master, float* grad, float* m, float* v, __nv_bfloat16* bf16_copy,
                  uint32_t count, uint32_t bf16_count, float lr, float beta1, float beta2, float eps,

@@ -123,6 +123,7 @@ FE_API fe_status fe_model_create(uint32_t seed, int device, fe_model** out) {
     };
     if (cudaMalloc(&m->master, mlp::kParams * 4) != cudaSuccess ||
         cudaMalloc(&m->grad, (mlp::kParams + 1) * 4) != cudaSuccess ||
+        cudaMalloc(&m->grad_part, (size_t)m->num_sms * (mlp::kParams + 1) * 4) != cudaSuccess ||
         cudaMalloc(&m->adam_m, mlp::kParams * 4) != cudaSuccess ||
         cudaMalloc(&m->adam_v, mlp::kParams * 4) != cudaSuccess ||
         cudaMalloc(&m->wbf16, mlp::kWeights * 2) != cudaSuccess ||
@@ -162,7 +163,8 @@ FE_API fe_status fe_model_destroy(fe_model* m) {
     if (!m) return FE_OK;
     cudaSetDevice(m->device);
     cudaDeviceSynchronize();
-    for (void* p : {(void*)m->master, (void*)m->grad, (void*)m->adam_m, (void*)m->adam_v,
+    for (void* p : {(void*)m->master, (void*)m->grad, (void*)m->grad_part, (void*)m->adam_m,
+                    (void*)m->adam_v,
                     (void*)m->wbf16, (void*)m->norm, (void*)m->flags, (void*)m->xb, (void*)m->ys})
         if (p) cudaFree(p);
     delete m;
@@ -259,8 +261,8 @@ static fe_status model_grads(fe_model* m, const float* d_x, const float* d_y, ui
     if (st != FE_OK) return st;
     k_standardize_y<<<(2 * n + 255) / 256, 256, 0, s>>>(d_y, m->norm, m->ys, n);
     M_CUDA(cudaGetLastError());
-    mlp::Grads G = mlp::grads_from(m->grad, m->grad + mlp::kParams);
-    M_CUDA(mlp::train_grads(m->params(), m->xb, m->ys, n, G, m->flags, s, m->num_sms));
+    M_CUDA(mlp::train_grads(m->params(), m->xb, m->ys, n, m->grad, m->grad_part, m->flags, s,
+                            m->num_sms));
     return FE_OK;
 }
 

@@ -14,6 +14,7 @@ struct fe_model {
     int num_sms = 148;
     float* master = nullptr;          // FP32 parameters (fe::mlp layout)
     float* grad = nullptr;            // gradients + 1 loss accumulator
+    float* grad_part = nullptr;       // per-block gradient slices [num_sms][kParams + 1]
     float* adam_m = nullptr;
     float* adam_v = nullptr;
     __nv_bfloat16* wbf16 = nullptr;   // BF16 weights for the tensor cores

@@ -139,6 +139,8 @@ class FeStats(Structure):
         ("total_divergence_iterations", c_uint64),
         ("flags", c_uint32),
         ("reserved", c_uint32),
+        ("density_residual_max", c_double),
+        ("divergence_residual_max", c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -164,6 +164,8 @@ typedef struct fe_stats {
     uint64_t total_divergence_iterations;
     uint32_t flags;                 /* FE_STATS_* bits                        */
     uint32_t reserved;
+    double density_residual_max;    /* largest per-particle error at exit,   */
+    double divergence_residual_max; /* same units as the residuals above      */
 } fe_stats;
 
 #define FE_STATS_ITERATION_CAP_HIT   0x1u /* a tolerance solve hit the cap   */

@@ -341,6 +341,7 @@ struct Base {
     virtual void viscosity() = 0;
     virtual void density_source() = 0;
     virtual void pressure_force() = 0;
+    double last_max = 0.0;  // largest per-particle error of the last residual pass
     virtual double pressure_update(bool want_residual, bool divergence) = 0;
     virtual void pressure_integration() = 0;
     virtual void divergence_source() = 0;
@@ -604,6 +605,11 @@ struct State : Base {
                 resid[i] = e > R(0) ? (double)e : 0.0;
             }
         }
+        if (want_residual) {
+            double mx = 0.0;
+            for (double v : resid) mx = std::max(mx, v);  // order-free
+            last_max = mx;
+        }
         return want_residual ? det_sum(resid.data(), n) : 0.0;
     }
 
@@ -819,7 +825,8 @@ double solver_metric(Base* s, double sum, bool divergence) {
 }
 
 // One Jacobi solve: fixed count, or the tolerance loop.
-uint32_t solve(Base* s, bool divergence, double* residual_out, bool* cap_hit) {
+uint32_t solve(Base* s, bool divergence, double* residual_out, bool* cap_hit,
+               double* residual_max_out) {
     const fe_params& p = s->p;
     if (p.solver == FE_SOLVER_FIXED_ITERS) {
         uint32_t k = divergence ? s->iters_div : s->iters_rho;
@@ -828,6 +835,7 @@ uint32_t solve(Base* s, bool divergence, double* residual_out, bool* cap_hit) {
             s->pressure_update(false, divergence);
         }
         *residual_out = 0.0;
+        *residual_max_out = 0.0;
         return k;
     }
     double tol = divergence ? (double)p.divergence_tolerance : (double)p.density_tolerance;
@@ -845,6 +853,9 @@ uint32_t solve(Base* s, bool divergence, double* residual_out, bool* cap_hit) {
         }
     }
     *residual_out = metric;
+    double mx = s->last_max;
+    if (divergence) mx = mx * (double)p.dt;
+    *residual_max_out = mx / (double)p.target_density;
     return it;
 }
 
@@ -852,7 +863,9 @@ void substep(Base* s, fe_stats* acc_stats, bool* cap_hit) {
     double r;
     s->viscosity();
     s->density_source();
-    uint32_t kr = solve(s, false, &r, cap_hit);
+    double rm = 0.0;
+    uint32_t kr = solve(s, false, &r, cap_hit, &rm);
+    acc_stats->density_residual_max = rm;
     acc_stats->density_iterations = kr;
     acc_stats->total_density_iterations += kr;
     acc_stats->density_residual = r;
@@ -860,7 +873,8 @@ void substep(Base* s, fe_stats* acc_stats, bool* cap_hit) {
     s->neighbor_search();
     s->density_alpha();
     s->divergence_source();
-    uint32_t kd = solve(s, true, &r, cap_hit);
+    uint32_t kd = solve(s, true, &r, cap_hit, &rm);
+    acc_stats->divergence_residual_max = rm;
     acc_stats->divergence_iterations = kd;
     acc_stats->total_divergence_iterations += kd;
     acc_stats->divergence_residual = r;

@@ -96,3 +96,20 @@ def test_model_save_and_load(trained, tmp_path):
     x = np.random.default_rng(0).normal(0, 1, (500, 12)).astype(np.float32)
     assert np.array_equal(learned.predict(trained.model, x), learned.predict(m2, x))
     m2.close()
+
+
+def test_long_cfl_run_stays_stable(trained):
+    """All 1000 frames of the 262k dam break with adaptive CFL (CFL number
+    0.3): the warm-started flow keeps the plain flow's largest speed (no
+    particle thrown out late in the run) and still needs far fewer
+    iterations to the same tolerance."""
+    res = learned.compare_iterations(trained.model, "dam_break_256k_cfl03", frames=998, warmup=2)
+    plain, lrn = res["plain"], res["learned"]
+    assert lrn["max_speed"] <= 1.5 * plain["max_speed"] + 1.0, (lrn["max_speed"],
+                                                                plain["max_speed"])
+    it_p = plain["density_iterations"] + plain["divergence_iterations"]
+    it_l = lrn["density_iterations"] + lrn["divergence_iterations"]
+    assert it_l <= it_p / 1.5, (it_l, it_p)
+    for arm in (plain, lrn):
+        assert arm["cap_hits"] == 0 and arm["non_finite"] == 0
+        assert arm["max_density_residual"] <= 1e-3 + 1e-9

@@ -170,7 +170,8 @@ def _run_frames(oracle_mod, p, pos, frames, substeps=1, flags=0, vel=None):
         for name in ("max_speed_bits", "density_error_fp", "divergence_error_fp",
                      "density_iterations", "divergence_iterations",
                      "avg_density_error_f64", "avg_divergence_error_f64",
-                     "density_residual", "divergence_residual", "dt"):
+                     "density_residual", "divergence_residual", "dt",
+                     "density_residual_max", "divergence_residual_max"):
             assert getattr(st, name) == getattr(rs, name), (f, name, getattr(st, name),
                                                            getattr(rs, name))
     compare_all(sim.data, orc, f"after {frames} frames")
