@@ -719,6 +719,63 @@ def run_profile_passes(args) -> None:
     sim.close()
 
 
+def run_profile_sort(args) -> None:
+    """A profiler-friendly sort: 2^22 uniform random 32-bit keys with a 32-bit
+    payload, sorted twice with 8-bit digits and 16 keys per thread; the second
+    sort runs inside the `profile_sort` NVTX range."""
+    import torch
+
+    from fluid_step import _abi
+    lib = _abi.load_library()
+    n = 1 << 22
+    rng = np.random.default_rng(1)
+    kd = torch.from_numpy(rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+                          .view(np.int32)).cuda()
+    vd = torch.arange(n, dtype=torch.int32, device="cuda")
+    for r in range(2):
+        k2, v2 = kd.clone(), vd.clone()
+        torch.cuda.synchronize()
+        if r == 1:
+            torch.cuda.nvtx.range_push("profile_sort")
+        _abi.check(lib, lib.fe_sort_pairs_config(ctypes.c_void_p(k2.data_ptr()),
+                                                 ctypes.c_void_p(v2.data_ptr()), n, 32, 8, 16,
+                                                 None), "fe_sort_pairs_config")
+        torch.cuda.synchronize()
+        if r == 1:
+            torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_sort": n}))
+
+
+def run_profile_render(args) -> None:
+    """The density splat and the water pass on the workload's state after 5
+    frames (1920x1080, camera 3 m above and 9 m in front of the box centre,
+    1024x512 synthetic sky); the second splat + raymarch run inside the
+    `profile_render` NVTX range."""
+    import torch
+
+    from fluid_step import camera, scene
+    from fluid_step.pipelines import Simulation
+    w = scene.workload(args.workload)
+    sim = Simulation(w.positions(), w.params)
+    for _ in range(5):
+        sim.step(1)
+    sim.data.set_skybox(camera.gradient_sky(1024, 512))
+    bmin, bmax = np.asarray(w.params.box_min), np.asarray(w.params.box_max)
+    c = (bmin + bmax) / 2
+    cam = camera.make_camera(c + np.array([0.0, 3.0, -9.0]), c, 1920, 1080)
+    for r in range(2):
+        torch.cuda.synchronize()
+        if r == 1:
+            torch.cuda.nvtx.range_push("profile_render")
+        g = sim.data.splat_density()
+        img = sim.data.raymarch(cam)
+        if r == 1:
+            torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_render": args.workload, "grid_sum": int(g.astype(np.uint64).sum()),
+                      "water_pixels": float((img[..., 3] > 0).mean())}))
+    sim.close()
+
+
 def run_reference(args) -> None:
     rank, world, _ = dist_env()
     if rank != 0:
@@ -766,6 +823,10 @@ def main():
                     help="learned warm start, plain Jacobi, or both (value = learned)")
     ap.add_argument("--profile-passes", action="store_true",
                     help="eager frames, then one launch of each hot pass (for ncu -k)")
+    ap.add_argument("--profile-sort", action="store_true",
+                    help="two 2^22 radix sorts, the second in an NVTX range (for ncu)")
+    ap.add_argument("--profile-render", action="store_true",
+                    help="splat + water pass twice on the workload, the second in an NVTX range")
     ap.add_argument("--eager", action="store_true",
                     help="launch frames without CUDA graphs (for profilers)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -780,6 +841,10 @@ def main():
         args.warmup = 3
     if args.profile_passes:
         run_profile_passes(args)
+    elif args.profile_sort:
+        run_profile_sort(args)
+    elif args.profile_render:
+        run_profile_render(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
