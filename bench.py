@@ -585,13 +585,28 @@ def run_gpu(args) -> None:
     alg = PASS_BYTES[dom] * n
     achieved = alg / (kern[dom] / 1e3) / 1e9
     traffic = None
+    warp_inst = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
         if dom in tj and tj[dom].get("workload") == args.workload:
             traffic = tj[dom]["dram_bytes_per_launch"]
+            warp_inst = tj[dom].get("warp_instructions_per_launch")
     except Exception:
         pass
+    # The neighbour-walk kernels are bound by instruction issue, not by HBM:
+    # warp instructions per launch (ncu smsp__inst_executed.sum) over the
+    # launch time, against 148 SMs x 4 schedulers x one issue per cycle at
+    # the SM clock sampled during the run.
+    issue = None
+    if warp_inst:
+        mhz = (head["clocks"] or {}).get("sm_mhz") or 1965.0
+        issue_peak = 148 * 4 * mhz * 1e6
+        issue_achieved = warp_inst / (kern[dom] / 1e3)
+        issue = {"kernel": dom, "warp_instructions_per_launch": warp_inst,
+                 "achieved": issue_achieved, "peak": issue_peak, "unit": "warp-inst/s",
+                 "frac": issue_achieved / issue_peak,
+                 "source": "instruction count from profiles/traffic.json (ncu)"}
 
     if rank == 0:
         cpu = None
@@ -626,6 +641,7 @@ def run_gpu(args) -> None:
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,
                          "launch_ms": kern[dom]},
+            "issue_roofline": issue,
             "kernel_ms": kern,
             "step_roofline": {"algorithmic_bytes_per_step": step_bytes(it_total, head["passes"]) * n,
                               "frac": step_bytes(it_total, head["passes"]) * n
@@ -699,6 +715,8 @@ def run_profile_passes(args) -> None:
     import torch
     for _ in range(3):
         sim.step(1, _abi.FE_STEP_NO_GRAPH)
+    for _ in range(args.profile_skip):       # further untimed frames (graph replays)
+        sim.step(1)
     lib, h = sim.data._lib, sim.data.handle
     lib.fe_synchronize(h)
     # Only the launches inside this range are of interest to a profiler
@@ -823,6 +841,8 @@ def main():
                     help="learned warm start, plain Jacobi, or both (value = learned)")
     ap.add_argument("--profile-passes", action="store_true",
                     help="eager frames, then one launch of each hot pass (for ncu -k)")
+    ap.add_argument("--profile-skip", type=int, default=0,
+                    help="with --profile-passes: frames to run before the profiled ones")
     ap.add_argument("--profile-sort", action="store_true",
                     help="two 2^22 radix sorts, the second in an NVTX range (for ncu)")
     ap.add_argument("--profile-render", action="store_true",

@@ -48,12 +48,17 @@ __device__ __forceinline__ int cell_coord(float p, float h) {
     return __float2int_rz(floorf(p / h));
 }
 
-// kernel_w (common.glsl:38-54).
-__device__ __forceinline__ float kernel_w(float r, float h) {
-    float q = r / h;
-    if (q >= 1.0f) return 0.0f;
+// 8 / (PI h^3), the normalisation of kernel_w and kernel_grad
+// (common.glsl:40, 58).  Hoisting it out of a neighbour loop repeats the
+// same two roundings, so the values are unchanged.
+__device__ __forceinline__ float kernel_norm(float h) {
     float h3 = h * h * h;
-    float k = 8.0f / (kPi * h3);
+    return 8.0f / (kPi * h3);
+}
+
+// kernel_w (common.glsl:38-54) for q = r / h and k = kernel_norm(h).
+__device__ __forceinline__ float kernel_w_q(float q, float k) {
+    if (q >= 1.0f) return 0.0f;
     if (q <= 0.5f) {
         float q2 = q * q;
         float q3 = q2 * q;
@@ -65,12 +70,10 @@ __device__ __forceinline__ float kernel_w(float r, float h) {
     }
 }
 
-// kernel_grad (common.glsl:56-73) as the scalar that multiplies r_vec.
-__device__ __forceinline__ float kernel_grad_scale(float r, float h) {
-    float q = r / h;
+// kernel_grad (common.glsl:56-73) as the scalar that multiplies r_vec, for
+// q = r / h and k = kernel_norm(h).
+__device__ __forceinline__ float kernel_grad_scale_q(float q, float r, float h, float k) {
     if (q >= 1.0f || r < kEpsR) return 0.0f;
-    float h3 = h * h * h;
-    float k = 8.0f / (kPi * h3);
     float gf;
     if (q <= 0.5f) {
         gf = k * (18.0f * q * q - 12.0f * q);
@@ -79,6 +82,16 @@ __device__ __forceinline__ float kernel_grad_scale(float r, float h) {
         gf = k * -6.0f * omq * omq;
     }
     return gf / (h * r);
+}
+
+// kernel_w (common.glsl:38-54).
+__device__ __forceinline__ float kernel_w(float r, float h) {
+    return kernel_w_q(r / h, kernel_norm(h));
+}
+
+// kernel_grad (common.glsl:56-73) as the scalar that multiplies r_vec.
+__device__ __forceinline__ float kernel_grad_scale(float r, float h) {
+    return kernel_grad_scale_q(r / h, r, h, kernel_norm(h));
 }
 
 // p / (rho * rho) for pressure_force, or NaN when rho <= 1e-6 (the shader

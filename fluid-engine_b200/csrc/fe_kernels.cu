@@ -123,15 +123,47 @@ __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
 // ---------------------------------------------------------------------------
 // density_and_alpha.comp:14-72 + neighbour list.
 //
-// Two phases with the shader's summation order.  Phase 1 walks the 27
-// buckets and only records the in-range candidates (r^2 <= h^2) in shared
-// memory: a short loop that the lanes of a warp execute together.  Phase 2
-// visits the recorded candidates in order and does the expensive part
-// (sqrt, kernel, gradient, list entry) with the lanes in lockstep.  A
-// particle with more than kStage in-range candidates redoes everything in a
-// single-phase walk.
+// Two phases with the shader's summation order.  Phase 1 finds the in-range
+// candidates (r^2 <= h^2, the shader's test) in walk order; phase 2 visits
+// them in that order and does the expensive part (sqrt, kernel, gradient,
+// list entry) with the lanes in lockstep.
+//
+// Phase 1 takes one of two forms, chosen per warp.  The lanes of a warp hold
+// consecutive particles of the sorted order, and a run of lanes whose
+// particles share a cell also shares that cell's 27 buckets.
+//  * Few runs (bulk fluid, several particles per cell): cell-cooperative.
+//    For each run the warp lays the 27 buckets end to end in walk order (z,
+//    y, x offsets, each bucket's entries in sorted order) and visits the
+//    candidates 32 at a time, one per lane: every lane tests its candidate
+//    against each particle of the run, and the ballot of the lanes that pass
+//    is that particle's in-range mask for the slab.  No lane idles on
+//    another's longer bucket, and a candidate's position is loaded once per
+//    run.  In phase 2 the set bits of a particle's masks, slab by slab and bit
+//    by bit, are its candidates in walk order; the run's table of non-empty
+//    buckets turns a bit back into a particle index.
+//  * Many runs (spray, sparse cells): each lane walks its own 27 buckets and
+//    records its in-range candidates.
+// A particle with more than kStage in-range candidates, or a run with more
+// than kMaxSlabs * 32 candidates, redoes everything in a single-phase walk.
 // ---------------------------------------------------------------------------
 constexpr int kStage = 44;
+constexpr int kMaxSlabs = 16;
+constexpr int kCoopRuns = 8;   // most runs per warp for the cooperative form
+
+struct RunTable {
+    uint32_t start[27];   // non-empty buckets in walk order: first entry
+    uint16_t excl[28];    // place of the bucket's first entry in the run's row; [K] = row length
+};
+
+// Per-warp scratch: one form or the other.
+union DensityScratch {
+    struct {
+        float4 pos[32];
+        uint32_t mask[kMaxSlabs][32];
+        RunTable table[kCoopRuns];
+    } coop;
+    uint32_t cand[kStage][32];
+};
 
 struct DensityAcc {
     float density = 0.0f, sum_grad_sq = 0.0f;
@@ -139,13 +171,16 @@ struct DensityAcc {
     uint32_t cnt = 0;
 };
 
-__device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, uint32_t j, f3 rv,
-                                             float r2, uint2* out, uint32_t stride) {
+// kn = kernel_norm(h); q = r / h is shared by W and grad W.
+__device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, float kn,
+                                             uint32_t j, f3 rv, float r2, uint2* out,
+                                             uint32_t stride) {
     float r = sqrtf(r2);
-    float w = kernel_w(r, h);
+    float q = r / h;
+    float w = kernel_w_q(q, kn);
     a.density += m * w;
     if (r > kEpsR) {
-        float g = kernel_grad_scale(r, h);
+        float g = kernel_grad_scale_q(q, r, h, kn);
         f3 grad = scale(g, rv);
         f3 mg = scale(m, grad);
         a.grad_sum = add(a.grad_sum, mg);
@@ -155,32 +190,154 @@ __device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, ui
     }
 }
 
+// Cooperative phase 1 over the runs of one warp (see above).  Returns, for
+// the calling lane, the table of its run (-1: single-phase walk) and its
+// number of in-range candidates.
+__device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& P,
+                                                DensityScratch& S, uint32_t heads, int n_live,
+                                                int cx, int cy, int cz, int& my_table,
+                                                uint32_t& n_in) {
+    const int lane = lane_id();
+    const float h = P.h;
+    const float h2 = h * h;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    int n_tables = 0;
+    while (heads) {
+        const int r0 = __ffs(heads) - 1;
+        heads &= heads - 1;
+        const int r1 = heads ? __ffs(heads) - 1 : n_live;
+        const int rx = __shfl_sync(kFull, cx, r0), ry = __shfl_sync(kFull, cy, r0),
+                  rz = __shfl_sync(kFull, cz, r0);
+        // lane t < 27: bucket t of the walk
+        uint32_t start = 0, len = 0;
+        if (lane < 27) {
+            const int x = lane % 3 - 1, y = (lane / 3) % 3 - 1, z = lane / 9 - 1;
+            const uint32_t k = P.table_base +
+                               cell_hash_pow2((int)((uint32_t)rx + (uint32_t)x),
+                                              (int)((uint32_t)ry + (uint32_t)y),
+                                              (int)((uint32_t)rz + (uint32_t)z), P.T - 1u);
+            const uint2 cell = B.cells[k];
+            if (cell.x != kEmpty) {
+                start = cell.x;
+                len = cell.y - cell.x;
+            }
+        }
+        uint32_t incl = len;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += v;
+        }
+        const uint32_t excl = incl - len;
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        const uint32_t nslab = (total + 31u) >> 5;
+        const bool mine = lane >= r0 && lane < r1;
+        if (nslab > (uint32_t)kMaxSlabs) continue;   // this run walks in phase 2
+        if (mine) my_table = n_tables;
+        RunTable& T = S.coop.table[n_tables++];
+        const uint32_t nonempty = __ballot_sync(kFull, len != 0);
+        if (len != 0) {
+            const int slot = __popc(nonempty & lt_mask);
+            T.start[slot] = start;
+            T.excl[slot] = (uint16_t)excl;
+        }
+        if (lane == 0) T.excl[__popc(nonempty)] = (uint16_t)total;
+        for (uint32_t sl = 0; sl < nslab; ++sl) {
+            const uint32_t cidx = (sl << 5) + (uint32_t)lane;
+            const bool valid = cidx < total;
+            // the bucket holding candidate cidx: the last t with excl_t <= cidx
+            int t = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int probe = t + step;
+                const uint32_t e = __shfl_sync(kFull, excl, probe & 31);
+                if (probe < 27 && e <= cidx) t = probe;
+            }
+            const uint32_t j =
+                __shfl_sync(kFull, start, t) + (cidx - __shfl_sync(kFull, excl, t));
+            const float4 q = valid ? __ldg(posb(B, j)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            uint32_t my_mask = 0;
+            for (int p = r0; p < r1; ++p) {
+                const float4 a = S.coop.pos[p];
+                const f3 rv = {a.x - q.x, a.y - q.y, a.z - q.z};
+                const float r2 = dot(rv, rv);
+                const uint32_t bits = __ballot_sync(kFull, valid && !(r2 > h2));
+                if (lane == p) my_mask = bits;
+            }
+            if (mine) {
+                S.coop.mask[sl][lane] = my_mask;
+                n_in += __popc(my_mask);
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
-    __shared__ uint32_t s_cand[kStage][kBlock];
+    __shared__ DensityScratch scratch[kBlock / 32];
     uint32_t i, s, c;
-    if (!chunk_of(B, i, s, c)) return;
+    const bool live = chunk_of(B, i, s, c);
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
-    const f3 pi = xyz(__ldg(posb(B, i)));
+    const float kn = kernel_norm(h);
+    const int lane = lane_id();
+    DensityScratch& S = scratch[threadIdx.x >> 5];
+    const float4 p4 = live ? __ldg(posb(B, i)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const f3 pi = xyz(p4);
+    const int cx = cell_coord(pi.x, h), cy = cell_coord(pi.y, h), cz = cell_coord(pi.z, h);
+
+    // Runs: live lanes form a prefix; a run starts where the cell changes.
+    const int px = __shfl_up_sync(kFull, cx, 1), py = __shfl_up_sync(kFull, cy, 1),
+              pz = __shfl_up_sync(kFull, cz, 1);
+    const bool head = live && (lane == 0 || cx != px || cy != py || cz != pz);
+    const uint32_t heads = __ballot_sync(kFull, head);
+    const int n_live = 32 - __clz(__ballot_sync(kFull, live));
+    const bool coop = __popc(heads) <= kCoopRuns;
+    int my_table = -1;
+    uint32_t n1 = 0;
+    if (coop) {
+        S.coop.pos[lane] = p4;
+        __syncwarp();
+        coop_candidates(B, P, S, heads, n_live, cx, cy, cz, my_table, n1);
+    } else if (live) {
+        walk(B, P, pi, [&](uint32_t j, f3, float) {
+            if (n1 < (uint32_t)kStage) S.cand[n1][lane] = j;
+            ++n1;
+        });
+    }
+    __syncwarp();
+    if (!live) return;
+
     uint2* out = B.nbr + i;
     const uint32_t stride = B.n_total;
-    const int t = threadIdx.x;
-    // Phase 1: in-range candidates in walk order.
-    uint32_t n1 = 0;
-    walk(B, P, pi, [&](uint32_t j, f3, float) {
-        if (n1 < (uint32_t)kStage) s_cand[n1][t] = j;
-        ++n1;
-    });
     DensityAcc a;
-    if (n1 <= (uint32_t)kStage) {
-        // Phase 2: the recorded candidates, same order.
+    if (coop && my_table >= 0) {
+        const RunTable& T = S.coop.table[my_table];
+        uint32_t sl = 0, bits = S.coop.mask[0][lane];
+        uint32_t t = 0, cur_start = T.start[0], cur_excl = 0, next_excl = T.excl[1];
         for (uint32_t k = 0; k < n1; ++k) {
-            uint32_t j = s_cand[k][t];
+            while (bits == 0) bits = S.coop.mask[++sl][lane];
+            const uint32_t cidx = (sl << 5) + (uint32_t)(__ffs(bits) - 1);
+            bits &= bits - 1;
+            while (cidx >= next_excl) {
+                ++t;
+                cur_start = T.start[t];
+                cur_excl = next_excl;
+                next_excl = T.excl[t + 1];
+            }
+            const uint32_t j = cur_start + (cidx - cur_excl);
             f3 rv = sub(pi, xyz(__ldg(posb(B, j))));
-            density_term(a, m, h, j, rv, dot(rv, rv), out, stride);
+            density_term(a, m, h, kn, j, rv, dot(rv, rv), out, stride);
+        }
+    } else if (!coop && n1 <= (uint32_t)kStage) {
+        for (uint32_t k = 0; k < n1; ++k) {
+            uint32_t j = S.cand[k][lane];
+            f3 rv = sub(pi, xyz(__ldg(posb(B, j))));
+            density_term(a, m, h, kn, j, rv, dot(rv, rv), out, stride);
         }
     } else {
-        walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) { density_term(a, m, h, j, rv, r2, out, stride); });
+        walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
+            density_term(a, m, h, kn, j, rv, r2, out, stride);
+        });
     }
     B.rho[i] = a.density;
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
