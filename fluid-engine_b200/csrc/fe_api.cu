@@ -1771,3 +1771,214 @@ fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Checkpoint / resume (no reference counterpart: GpuPhysicsData,
+// particle.rs:137-308, lives only as long as its Vulkan buffers).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr char kStateMagic[8] = {'F', 'E', 'S', 'T', 'A', 'T', 'E', '\0'};
+
+struct StateHeader {
+    char magic[8];
+    uint32_t version, abi;
+    uint32_t n, T, n_scenes, has_carry;
+    uint32_t initialized, last_substeps;
+    uint32_t size_params, size_devparams, size_scene, size_global;
+    uint64_t bytes;  // the whole snapshot
+};
+
+struct Section {
+    void* dev;
+    size_t bytes;
+};
+
+// Device-resident state in snapshot order (after the header and the host
+// parameter blocks).
+std::vector<Section> state_sections(const fe_ctx* c, bool carry) {
+    const size_t n = c->n, T = c->T, ns = c->B.n_scenes;
+    const Bufs& B = c->B;
+    std::vector<Section> v = {{B.P, sizeof(DevParams) * ns},
+                              {B.S, sizeof(SceneState) * ns},
+                              {B.G, sizeof(GlobalState)},
+                              {B.pos_a, n * 16},
+                              {B.vel_a, n * 16},
+                              {B.pos_b, n * 16},
+                              {B.vel_b, n * 16},
+                              {B.rec, n * 32},
+                              {B.rho, n * 4},
+                              {B.alpha, n * 4},
+                              {B.src, n * 4},
+                              {B.prs, n * 4},
+                              {B.keys, T * 4},
+                              {B.vals, T * 4},
+                              {B.cells, T * 8}};
+    if (carry) v.push_back({c->L.carry, n * 16});
+    return v;
+}
+
+size_t state_bytes(const fe_ctx* c, bool carry) {
+    size_t b = sizeof(StateHeader) + sizeof(fe_params) * c->B.n_scenes;
+    for (const Section& s : state_sections(c, carry)) b += s.bytes;
+    return b;
+}
+
+// The learned warm start's carried state as a fresh context has it.
+fe_status reset_carry(fe_ctx* c) {
+    FE_CUDA(cudaMemsetAsync(c->L.carry, 0, (size_t)c->n * 16, c->stream));
+    FE_CUDA(cudaMemset2DAsync(reinterpret_cast<char*>(c->L.carry) + 12, 16, 0xFF, 4, c->n,
+                              c->stream));
+    return FE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+FE_API fe_status fe_state_size(const fe_ctx* c, size_t* bytes) {
+    if (!c || !bytes) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    *bytes = state_bytes(c, c->L.carry != nullptr);
+    return FE_OK;
+}
+
+FE_API fe_status fe_state_export(fe_ctx* c, void* dst, size_t bytes) {
+    if (!c || !dst) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    const bool carry = c->L.carry != nullptr;
+    const size_t need = state_bytes(c, carry);
+    if (bytes < need) {
+        set_error("snapshot needs %zu bytes, buffer has %zu", need, bytes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    const uint32_t ns = c->B.n_scenes;
+    StateHeader hd;
+    std::memset(&hd, 0, sizeof hd);
+    std::memcpy(hd.magic, kStateMagic, sizeof hd.magic);
+    hd.version = FE_STATE_VERSION;
+    hd.abi = FE_ABI_VERSION;
+    hd.n = c->n;
+    hd.T = c->T;
+    hd.n_scenes = ns;
+    hd.has_carry = carry ? 1u : 0u;
+    hd.initialized = c->initialized ? 1u : 0u;
+    hd.last_substeps = c->last_substeps;
+    hd.size_params = sizeof(fe_params);
+    hd.size_devparams = sizeof(DevParams);
+    hd.size_scene = sizeof(SceneState);
+    hd.size_global = sizeof(GlobalState);
+    hd.bytes = need;
+    char* out = static_cast<char*>(dst);
+    std::memcpy(out, &hd, sizeof hd);
+    char* host_params = out + sizeof hd;
+    char* p = host_params + sizeof(fe_params) * ns;
+    char* dev_params = p;
+    for (const Section& s : state_sections(c, carry)) {
+        FE_CUDA(cudaMemcpyAsync(p, s.dev, s.bytes, cudaMemcpyDeviceToHost, c->stream));
+        p += s.bytes;
+    }
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    // the parameter blocks with dt as the device last set it (adaptive CFL)
+    for (uint32_t k = 0; k < ns; ++k) {
+        fe_params q = c->params[k];
+        DevParams dp;
+        std::memcpy(&dp, dev_params + sizeof(DevParams) * k, sizeof dp);
+        q.dt = dp.dt;
+        std::memcpy(host_params + sizeof(fe_params) * k, &q, sizeof q);
+    }
+    return FE_OK;
+}
+
+FE_API fe_status fe_state_import(fe_ctx* c, const void* src, size_t bytes) {
+    if (!c || !src) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    StateHeader hd;
+    if (bytes < sizeof hd) {
+        set_error("snapshot of %zu bytes is shorter than its header", bytes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    std::memcpy(&hd, src, sizeof hd);
+    const uint32_t ns = c->B.n_scenes;
+    if (std::memcmp(hd.magic, kStateMagic, sizeof hd.magic) != 0 || hd.version != FE_STATE_VERSION ||
+        hd.abi != FE_ABI_VERSION || hd.size_params != sizeof(fe_params) ||
+        hd.size_devparams != sizeof(DevParams) || hd.size_scene != sizeof(SceneState) ||
+        hd.size_global != sizeof(GlobalState) || hd.has_carry > 1u) {
+        set_error("not a snapshot of this library version");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (hd.n != c->n || hd.T != c->T || hd.n_scenes != ns) {
+        set_error("snapshot of %u particles / %u slots / %u scenes, context has %u / %u / %u",
+                  hd.n, hd.T, hd.n_scenes, c->n, c->T, ns);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    const bool carry = hd.has_carry != 0;
+    const size_t need = state_bytes(c, carry);
+    if (hd.bytes != need || bytes < need) {
+        set_error("snapshot should hold %zu bytes (header says %llu, buffer has %zu)", need,
+                  (unsigned long long)hd.bytes, bytes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    const char* in = static_cast<const char*>(src);
+    const char* host_params = in + sizeof hd;
+    const char* dev_params = host_params + sizeof(fe_params) * ns;
+    std::vector<fe_params> params(ns);
+    std::vector<DevParams> dparams(ns);
+    for (uint32_t k = 0; k < ns; ++k) {
+        std::memcpy(&params[k], host_params + sizeof(fe_params) * k, sizeof(fe_params));
+        std::memcpy(&dparams[k], dev_params + sizeof(DevParams) * k, sizeof(DevParams));
+        fe_status s = validate(&params[k]);
+        if (s != FE_OK) return s;
+        const DevParams& a = dparams[k];
+        const DevParams& b = c->dparams[k];
+        if (a.n != b.n || a.T != b.T || a.table_base != b.table_base || a.first != b.first) {
+            set_error("scene %u: snapshot layout differs from the context's", k);
+            return FE_ERR_INVALID_ARGUMENT;
+        }
+    }
+    if (ns > 1 && params[0].sort_algorithm != FE_SORT_RADIX) {
+        set_error("bitonic sort is single-scene only");
+        return FE_ERR_UNSUPPORTED;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    fe_status s = FE_OK;
+    if (carry && (s = ensure_learn_buffers(c)) != FE_OK) return s;
+    drop_graphs(c);
+    const char* p = dev_params;
+    const char* global = nullptr;
+    for (const Section& sec : state_sections(c, carry)) {
+        if (sec.dev == c->B.G)
+            global = p;
+        else
+            FE_CUDA(cudaMemcpyAsync(sec.dev, p, sec.bytes, cudaMemcpyHostToDevice, c->stream));
+        p += sec.bytes;
+    }
+    if (!carry && c->L.carry && (s = reset_carry(c)) != FE_OK) return s;
+    // The neighbour list is not part of a snapshot.  The last pass that
+    // built it (density_alpha after the frame's last neighbour search) read
+    // only the restored positions and cell table, so running it again
+    // rebuilds the same list and rewrites the same densities, factors and
+    // p / rho^2.  The global flags are restored after it.
+    if (hd.initialized) {
+        Recorder R = eager(c);
+        if ((s = rec_simple(c, R, k_density_alpha)) != FE_OK) return s;
+    }
+    FE_CUDA(cudaMemcpyAsync(c->B.G, global, sizeof(GlobalState), cudaMemcpyHostToDevice,
+                            c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    c->params = params;
+    c->dparams = dparams;
+    c->initialized = hd.initialized != 0;
+    c->last_substeps = hd.last_substeps;
+    c->prepared = true;
+    return FE_OK;
+}
+
+}  // extern "C"

@@ -13,6 +13,7 @@ from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
                     c_int32, c_size_t, c_uint32, c_uint64, c_void_p)
 
 ABI_VERSION = 1
+FE_STATE_VERSION = 1
 
 # fe_status
 FE_OK = 0
@@ -316,6 +317,9 @@ SIGNATURES = {
     "fe_divergence_integration": (c_int, [CTX]),
     "fe_stats_pass": (c_int, [CTX]),
     "fe_read_stats": (c_int, [CTX, POINTER(FeStats)]),
+    "fe_state_size": (c_int, [CTX, POINTER(c_size_t)]),
+    "fe_state_export": (c_int, [CTX, c_void_p, c_size_t]),
+    "fe_state_import": (c_int, [CTX, c_void_p, c_size_t]),
     "fe_step": (c_int, [CTX, c_uint32, c_uint32, POINTER(FeStats)]),
     "fe_sort_pairs": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p]),
     "fe_sort_pairs_host": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int]),

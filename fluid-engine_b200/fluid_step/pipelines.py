@@ -86,6 +86,21 @@ class GpuPhysicsData:
         check(self._lib, self._lib.fe_read_stats(self.handle, ctypes.byref(st)), "fe_read_stats")
         return st
 
+    # -- checkpoint / resume (fe_state_export / fe_state_import) --------------
+    def export_state(self) -> bytes:
+        """A snapshot of everything a later step reads (versioned binary)."""
+        size = ctypes.c_size_t()
+        check(self._lib, self._lib.fe_state_size(self.handle, ctypes.byref(size)), "fe_state_size")
+        buf = ctypes.create_string_buffer(size.value)
+        check(self._lib, self._lib.fe_state_export(self.handle, buf, size.value), "fe_state_export")
+        return buf.raw
+
+    def import_state(self, snapshot: bytes) -> None:
+        """Restores a snapshot of a context with the same sizes and scene layout."""
+        buf = ctypes.create_string_buffer(bytes(snapshot), len(snapshot))
+        check(self._lib, self._lib.fe_state_import(self.handle, buf, len(snapshot)),
+              "fe_state_import")
+
     # -- density_texture.rs / splat_density.comp -----------------------------
     def splat_density(self) -> np.ndarray:
         """Clears and splats the headless density grid (fe_density_splat);

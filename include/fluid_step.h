@@ -353,6 +353,35 @@ FE_API fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
 FE_API fe_status fe_read_scene_stats(fe_ctx* ctx, uint32_t scene, fe_stats* out);
 
 /* ------------------------------------------------------------------------- */
+/* Checkpoint / resume                                                       */
+/* ------------------------------------------------------------------------- */
+/* The reference keeps its state in GpuPhysicsData's buffers
+ * (particle.rs:137-308) and has no checkpoint; these entry points snapshot
+ * everything a later fe_step reads, so that a context restored from a
+ * snapshot continues bit for bit as the original would have:
+ *   a versioned header (magic "FESTATE", FE_STATE_VERSION, ABI version,
+ *   particle and table sizes, scene count, struct sizes), the parameter
+ *   block of every scene, the device-side scene parameters (dt as adaptive
+ *   CFL last set it) and solver state (stats, iteration totals, last
+ *   residuals), and the per-particle arrays: position_a/b, velocity_a/b,
+ *   pressure acceleration, density, factor, source term, pressure, the grid
+ *   entries and cell starts, and the learned warm start's carried
+ *   pressures when the context has them.
+ * The snapshot is host memory in native byte order.  The neighbour list is
+ * not part of it: the import rebuilds it with the density pass that built it
+ * last, on the restored positions and cell table.
+ * fe_state_size: bytes of a snapshot of this context.
+ * fe_state_export: writes it; `bytes` must be at least fe_state_size.
+ * fe_state_import: restores one into a context with the same particle count,
+ *   table size and scene layout (FE_ERR_INVALID_ARGUMENT otherwise, and for a
+ *   damaged header or a short buffer; the context is then unchanged).
+ *   Recorded frame graphs are dropped.  An attached model stays attached. */
+#define FE_STATE_VERSION 1u
+FE_API fe_status fe_state_size(const fe_ctx* ctx, size_t* bytes);
+FE_API fe_status fe_state_export(fe_ctx* ctx, void* dst, size_t bytes);
+FE_API fe_status fe_state_import(fe_ctx* ctx, const void* src, size_t bytes);
+
+/* ------------------------------------------------------------------------- */
 /* Whole step                                                                */
 /* ------------------------------------------------------------------------- */
 /* One frame of the physics half of `Renderer::step` (renderer/mod.rs:

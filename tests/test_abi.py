@@ -141,3 +141,10 @@ def test_sort_config_rejects_non_candidates(lib):
     # shape validation happens before any device work
     assert lib.fe_sort_pairs_config(None, None, 0, 32, 9, 8, None) == _abi.FE_ERR_INVALID_ARGUMENT
     assert lib.fe_sort_pairs_config(None, None, 0, 32, 8, 5, None) == _abi.FE_ERR_INVALID_ARGUMENT
+
+
+def test_state_calls_reject_null(lib):
+    size = ctypes.c_size_t()
+    assert lib.fe_state_size(None, ctypes.byref(size)) == _abi.FE_ERR_INVALID_ARGUMENT
+    assert lib.fe_state_export(None, None, 0) == _abi.FE_ERR_INVALID_ARGUMENT
+    assert lib.fe_state_import(None, None, 0) == _abi.FE_ERR_INVALID_ARGUMENT
