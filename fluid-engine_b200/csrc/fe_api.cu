@@ -11,7 +11,10 @@
 // any host round trip.
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -34,6 +37,17 @@
 #include "fe_tune.h"
 
 using namespace fe;
+
+// An NVTX range around each entry point that records or launches GPU work
+// (the reference wraps each ComputeStep::execute in a Tracy span,
+// renderer/mod.rs:279-340).  Like those spans, a range covers the host-side
+// recording and launch; the device time is in the profiler's kernel rows.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 namespace {
 
@@ -305,14 +319,30 @@ struct fe_ctx {
 
 namespace {
 
+// Test hooks (fe_debug_fail_allocation, fe_debug_poison_allocations).
+std::atomic<uint32_t> g_fail_countdown{0};
+std::atomic<int> g_poison{0};
+
 template <class T>
 fe_status dev_alloc(fe_ctx* c, T** out, size_t count) {
     void* p = nullptr;
     size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    uint32_t k = g_fail_countdown.load();
+    while (k != 0 && !g_fail_countdown.compare_exchange_weak(k, k - 1)) {
+    }
+    if (k == 1) {
+        set_error("device allocation of %zu bytes failed (injected)", bytes);
+        return FE_ERR_OUT_OF_MEMORY;
+    }
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
         set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
         return FE_ERR_OUT_OF_MEMORY;
+    }
+    if (g_poison.load() && cudaMemset(p, 0xFF, bytes) != cudaSuccess) {
+        cudaFree(p);
+        set_error("poisoning a new allocation failed");
+        return FE_ERR_CUDA;
     }
     c->allocations.push_back(p);
     *out = static_cast<T*>(p);
@@ -1130,6 +1160,7 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
 
 #define FE_STAGE(name, body)                                 \
     fe_status name(fe_ctx* c) {                              \
+        NvtxRange range_(#name);                             \
         fe_status s_ = need_prepared(c, #name);              \
         if (s_ != FE_OK) return s_;                          \
         Recorder R = eager(c);                               \
@@ -1160,6 +1191,7 @@ FE_STAGE(fe_stats_pass, return rec_stats(c, R))
 // (renderer/mod.rs:385-390; density_texture.rs; splat_density.comp) into the
 // context's headless grid.
 fe_status fe_density_splat(fe_ctx* c) {
+    NvtxRange range_("fe_density_splat");
     if (!c) {
         set_error("context is NULL");
         return FE_ERR_INVALID_ARGUMENT;
@@ -1256,6 +1288,7 @@ fe_status fe_set_skybox(fe_ctx* c, const float* rgba, uint32_t width, uint32_t h
 // The water pass (water_pipeline.rs; raymarch.vert/.frag) of the last
 // fe_density_splat grid into the context's RGBA32F image.
 fe_status fe_raymarch(fe_ctx* c, const fe_camera* cam) {
+    NvtxRange range_("fe_raymarch");
     if (!c || !cam) {
         set_error("NULL argument");
         return FE_ERR_INVALID_ARGUMENT;
@@ -1324,6 +1357,7 @@ fe_status fe_read_scene_stats(fe_ctx* c, uint32_t scene, fe_stats* out) {
 }
 
 fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {
+    NvtxRange range_("fe_step");
     fe_status s = need_prepared(c, "fe_step");
     if (s != FE_OK) return s;
     if (n_substeps > 1024) {
@@ -1572,6 +1606,7 @@ fe_status sort_pairs_impl(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t k
 
 fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key_bits,
                         int algorithm, void* stream_ptr) {
+    NvtxRange range_("fe_sort_pairs");
     return sort_pairs_impl(keys, vals, n, key_bits, algorithm, stream_ptr, nullptr);
 }
 
@@ -1978,6 +2013,32 @@ FE_API fe_status fe_state_import(fe_ctx* c, const void* src, size_t bytes) {
     c->initialized = hd.initialized != 0;
     c->last_substeps = hd.last_substeps;
     c->prepared = true;
+    return FE_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Test hooks.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+FE_API void fe_debug_fail_allocation(uint32_t k) { g_fail_countdown.store(k); }
+
+FE_API void fe_debug_poison_allocations(int on) { g_poison.store(on ? 1 : 0); }
+
+FE_API fe_status fe_debug_bounded_wait(int device, uint32_t limit, uint32_t* flags) {
+    if (!flags || limit == 0) {
+        set_error("fe_debug_bounded_wait needs flags and a non-zero limit");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    *flags = 0;
+    FE_CUDA(cudaSetDevice(device));
+    FE_CUDA(lookback_wait_selftest((int)std::min<uint32_t>(limit, 1u << 30), flags));
+    if (*flags & 0x4u) {
+        set_error("a bounded device wait timed out (look-back)");
+        return FE_ERR_TIMEOUT;
+    }
     return FE_OK;
 }
 

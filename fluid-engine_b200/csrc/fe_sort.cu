@@ -44,6 +44,17 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// One more poll of a look-back wait: false, with the look-back timeout flag
+// raised, once `limit` polls are spent.
+__device__ __forceinline__ bool lookback_backoff(int& spins, int limit, uint32_t* error_flags) {
+    if (++spins > limit) {
+        atomicOr(error_flags, 0x4u);
+        return false;
+    }
+    __nanosleep(32);
+    return true;
+}
+
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -239,13 +250,7 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<kBits, kItems>()) k_
                     if (flag == kFlagInc) done = true;
                 }
                 pred -= used;
-                if (stalled && !done) {
-                    if (++spins > kMaxSpins) {
-                        atomicOr(error_flags, 0x4u);
-                        break;
-                    }
-                    __nanosleep(32);
-                }
+                if (stalled && !done && !lookback_backoff(spins, kMaxSpins, error_flags)) break;
             }
             atomicExch(status + (size_t)tile * kDig + d, kFlagInc | (excl + count[j]));
         }
@@ -446,6 +451,29 @@ cudaError_t radix_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint
     }
     *result_in_tmp = (passes % 2) == 1;
     return cudaSuccess;
+}
+
+namespace {
+// A look-back wait on a status word that no block ever publishes: it gives
+// up after `limit` polls through the same backoff as the radix pass.
+__global__ void k_lookback_selftest(const uint32_t* status, uint32_t* error_flags, int limit) {
+    int spins = 0;
+    while ((ld_volatile(status) & ~kValueMask) == 0)
+        if (!lookback_backoff(spins, limit, error_flags)) break;
+}
+}  // namespace
+
+cudaError_t lookback_wait_selftest(int limit, uint32_t* flags_out) {
+    uint32_t* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 8);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemset(d, 0, 8)) == cudaSuccess) {
+        k_lookback_selftest<<<1, 1>>>(d, d + 1, limit < kMaxSpins ? limit : kMaxSpins);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(flags_out, d + 1, 4, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d);
+    return e;
 }
 
 cudaError_t bitonic_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint32_t n) {

@@ -63,4 +63,9 @@ cudaError_t radix_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint
 // In-place bitonic network; n must be a power of two.
 cudaError_t bitonic_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint32_t n);
 
+// Runs one look-back wait on a status word that is never published, with at
+// most `limit` polls (clamped to the radix pass's own limit), on the current
+// device; *flags_out receives the error flags it raised (0x4 = timed out).
+cudaError_t lookback_wait_selftest(int limit, uint32_t* flags_out);
+
 }  // namespace fe

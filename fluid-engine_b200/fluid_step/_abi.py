@@ -317,6 +317,9 @@ SIGNATURES = {
     "fe_divergence_integration": (c_int, [CTX]),
     "fe_stats_pass": (c_int, [CTX]),
     "fe_read_stats": (c_int, [CTX, POINTER(FeStats)]),
+    "fe_debug_fail_allocation": (None, [c_uint32]),
+    "fe_debug_poison_allocations": (None, [c_int]),
+    "fe_debug_bounded_wait": (c_int, [c_int, c_uint32, POINTER(c_uint32)]),
     "fe_state_size": (c_int, [CTX, POINTER(c_size_t)]),
     "fe_state_export": (c_int, [CTX, c_void_p, c_size_t]),
     "fe_state_import": (c_int, [CTX, c_void_p, c_size_t]),

@@ -382,6 +382,27 @@ FE_API fe_status fe_state_export(fe_ctx* ctx, void* dst, size_t bytes);
 FE_API fe_status fe_state_import(fe_ctx* ctx, const void* src, size_t bytes);
 
 /* ------------------------------------------------------------------------- */
+/* Test hooks                                                                */
+/* ------------------------------------------------------------------------- */
+/* The reference has no failure handling (it panics, density_alpha.rs:57,
+ * sorter.rs:57-60); these hooks let tests drive this library's error paths
+ * without faulting a GPU.  They are process-wide and not thread-safe with
+ * respect to concurrent context creation.
+ * fe_debug_fail_allocation(k): the k-th device allocation of a context
+ *   (fe_create, fe_batch_create and the buffers contexts add later) from now
+ *   on fails with FE_ERR_OUT_OF_MEMORY; 0 turns the hook off.
+ * fe_debug_poison_allocations(on): new context allocations are filled with
+ *   0xFF bytes (NaN as floats, 0xFFFFFFFF as indices), so that a read of
+ *   memory no pass has written shows up in the results.
+ * fe_debug_bounded_wait(device, limit, flags): runs one look-back wait of
+ *   the radix pass on a status word that is never published, giving up
+ *   after `limit` polls; returns FE_ERR_TIMEOUT with FE_STATS_LOOKBACK_TIMEOUT
+ *   in *flags, and the device stays usable. */
+FE_API void fe_debug_fail_allocation(uint32_t k);
+FE_API void fe_debug_poison_allocations(int on);
+FE_API fe_status fe_debug_bounded_wait(int device, uint32_t limit, uint32_t* flags);
+
+/* ------------------------------------------------------------------------- */
 /* Whole step                                                                */
 /* ------------------------------------------------------------------------- */
 /* One frame of the physics half of `Renderer::step` (renderer/mod.rs:

@@ -148,3 +148,11 @@ def test_state_calls_reject_null(lib):
     assert lib.fe_state_size(None, ctypes.byref(size)) == _abi.FE_ERR_INVALID_ARGUMENT
     assert lib.fe_state_export(None, None, 0) == _abi.FE_ERR_INVALID_ARGUMENT
     assert lib.fe_state_import(None, None, 0) == _abi.FE_ERR_INVALID_ARGUMENT
+
+
+def test_debug_hooks_validate_before_device_work(lib):
+    flags = ctypes.c_uint32()
+    assert lib.fe_debug_bounded_wait(0, 0, ctypes.byref(flags)) == _abi.FE_ERR_INVALID_ARGUMENT
+    assert lib.fe_debug_bounded_wait(0, 10, None) == _abi.FE_ERR_INVALID_ARGUMENT
+    lib.fe_debug_fail_allocation(0)
+    lib.fe_debug_poison_allocations(0)
