@@ -111,6 +111,15 @@ __device__ __forceinline__ float4* accp(const Bufs& B, uint32_t i) {
     return B.rec + 2 * (size_t)i + 1;
 }
 
+// Both halves of particle i's record in one 256-bit store: the 32-byte sector
+// is written whole, so L2 never merges a half-written sector with DRAM.
+__device__ __forceinline__ void st_record(const Bufs& B, uint32_t i, float4 pos, float4 acc) {
+    float4* p = B.rec + 2 * (size_t)i;
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(pos.x),
+                 "f"(pos.y), "f"(pos.z), "f"(pos.w), "f"(acc.x), "f"(acc.y), "f"(acc.z), "f"(acc.w)
+                 : "memory");
+}
+
 // Both halves of particle j's record in one 256-bit read-only load.
 __device__ __forceinline__ void ld_record(const Bufs& B, uint32_t j, float4& pos, float4& acc) {
     const float4* p = B.rec + 2 * (size_t)j;

@@ -78,8 +78,9 @@ struct Bufs {
     // position_b; w holds p / rho^2 (NaN when rho <= 1e-6) for pressure_force.
     float4* pos_b;
     // 32-byte record per particle: rec[2i] = copy of position_b (xyz),
-    // rec[2i+1] = pressure acceleration.  pressure_update fetches both halves
-    // of a neighbour with one 256-bit load.
+    // rec[2i+1] = pressure acceleration, both written by pressure_force with
+    // one 256-bit store.  pressure_update fetches both halves of a neighbour
+    // with one 256-bit load.
     float4* rec;
     float *rho, *alpha, *src, *prs, *prs_tmp;
     uint32_t *keys, *vals;      // grid_entries (hash, index), T_total

@@ -66,6 +66,9 @@ __global__ void k_offsets(Bufs B) {
 // The neighbour list of the old order is invalidated: until density_alpha
 // rebuilds it, the neighbour passes walk the new buckets.
 // kCarry: the learned warm start's per-particle state is gathered too.
+// Every store is a whole aligned vector of a fully written array (no
+// read-modify-write of pos_b, no half-written record): partial sectors
+// made this pass about twice as slow.
 template <bool kCarry>
 __device__ __forceinline__ void reorder_body(const Bufs& B, int carry_pressure,
                                              const LearnArgs& L) {
@@ -75,11 +78,12 @@ __device__ __forceinline__ void reorder_body(const Bufs& B, int carry_pressure,
     if (src >= B.n_total) src = i;  // unreachable for a valid permutation
     B.nbr_count[i] = kNbrCap + 1;
     // pos_b.w holds p / rho^2 of slot i (pressures and densities are not
-    // permuted here), so it is carried over.
+    // permuted here): the value every pass that writes p or rho maintains,
+    // recomputed from them.  The records' position half is written by
+    // pressure_force, the only pass before pressure_update that needs it.
     float4 p = __ldg(B.pos_a + src);
-    p.w = posb(B, i)->w;
+    p.w = pressure_over_rho2(B.prs[i], B.rho[i]);
     *posb(B, i) = p;
-    *rec_pos(B, i) = p;
     B.vel_b[i] = __ldg(B.vel_a + src);
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
     if (kCarry) L.carry_tmp[i] = L.carry[src];
@@ -468,7 +472,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which)
     if (which >= 0 && B.S[s].solve[which].done) return;
     const DevParams& P = B.P[s];
     const float m = P.mass;
-    const f3 pi = xyz(__ldg(posb(B, i)));
+    const float4 p4 = __ldg(posb(B, i));
+    const f3 pi = xyz(p4);
     const float rho_i = B.rho[i], p_i = B.prs[i];
     float p_rho_i = 0.0f;
     if (rho_i > kEpsR) p_rho_i = p_i / (rho_i * rho_i);
@@ -483,7 +488,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which)
                 acc = add(acc, scale(m * term, grad));
             }
         });
-    *accp(B, i) = make_float4(-acc.x, -acc.y, -acc.z, 0.0f);
+    // the whole record: this particle's position for pressure_update's
+    // gathers and its acceleration
+    st_record(B, i, p4, make_float4(-acc.x, -acc.y, -acc.z, 0.0f));
 }
 
 // ---------------------------------------------------------------------------
