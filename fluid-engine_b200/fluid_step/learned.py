@@ -121,7 +121,13 @@ def capture(workload_names=("dam_break_16k", "dam_break_256k"), frames=(100, 300
         xs.append(x[:k])
         ys.append(y[:k])
         sim.close()
-    return np.concatenate(xs), np.concatenate(ys)
+    x, y = np.concatenate(xs), np.concatenate(ys)
+    # Which samples are taken is fixed by a hash of (particle, substep,
+    # solve), but their slots come from a device atomic counter, so the row
+    # order varies from run to run.  A canonical order (lexicographic over
+    # the row's values) makes training, and everything after it, repeatable.
+    order = np.lexsort(np.concatenate([x, y], axis=1).T[::-1])
+    return x[order], y[order]
 
 
 def train(x: np.ndarray, y: np.ndarray, *, epochs: int = 30, batch: int = 4096,
