@@ -1124,8 +1124,10 @@ fe_status fe_upload(fe_ctx* c, fe_field f, const void* src, size_t bytes) {
     if (f == FE_FIELD_POSITION_B)  // keep pressure_update's copy in the records
         FE_CUDA(cudaMemcpy2DAsync(c->B.rec, 32, src, 16, 16, c->n, cudaMemcpyHostToDevice,
                                   c->stream));
-    // pos_b.w caches p / rho^2 for pressure_force.
-    if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY || f == FE_FIELD_POSITION_B)
+    // pos_b.w caches p / rho^2 for pressure_force, velocity_b.w rho for
+    // viscosity.
+    if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY || f == FE_FIELD_POSITION_B ||
+        f == FE_FIELD_VELOCITY_B)
         return run_refresh_pr(c);
     return FE_OK;
 }
@@ -1154,6 +1156,12 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
         // pressure_integration.comp:75).
         float* v = static_cast<float*>(dst);
         for (uint32_t i = 0; i < c->n; ++i) v[4 * i + 3] = 1.0f;
+    }
+    if (f == FE_FIELD_VELOCITY_B) {
+        // The device keeps the density in w; the reference's velocity_b.w is
+        // the copied velocity_a.w, which its passes always write as 0.
+        float* v = static_cast<float*>(dst);
+        for (uint32_t i = 0; i < c->n; ++i) v[4 * i + 3] = 0.0f;
     }
     return FE_OK;
 }

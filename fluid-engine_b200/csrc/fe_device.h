@@ -74,6 +74,8 @@ enum Ticket : int { kTicketStats = 0, kTicketSolve = 1, kTicketHist = 2 };
 
 // Kernel-side view of every buffer of a context (passed by value).
 struct Bufs {
+    // velocity_b.w holds the slot's density (written by density_alpha, kept by
+    // the FIXED-mode divergence integration) for viscosity's gathers.
     float4 *pos_a, *vel_a, *vel_b;
     // position_b; w holds p / rho^2 (NaN when rho <= 1e-6) for pressure_force.
     float4* pos_b;

@@ -117,11 +117,13 @@ __global__ void __launch_bounds__(kBlock) k_take_pressure_carry(Bufs B, LearnArg
     take_pressure_body<true>(B, L);
 }
 
-// pr = p / rho^2 for all particles (after a host upload of p or rho).
+// pr = p / rho^2 and velocity_b.w = rho for all particles (after a host
+// upload of p, rho, position_b or velocity_b).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
     posb(B, i)->w = pressure_over_rho2(B.prs[i], B.rho[i]);
+    B.vel_b[i].w = B.rho[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -344,6 +346,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
         });
     }
     B.rho[i] = a.density;
+    // velocity_b.w carries the density for viscosity's neighbour gathers
+    B.vel_b[i].w = a.density;
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
     B.alpha[i] = al > kEpsR ? al : 0.0f;
     B.nbr_count[i] = a.cnt;
@@ -362,18 +366,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
     const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(B.vel_b + i));
     f3 sum = {0.0f, 0.0f, 0.0f};
-    struct VR {
-        float4 v;
-        float rho;
-    };
+    // velocity_b.w = rho_j (written by density_alpha): one gather per neighbour
     for_each_neighbor(
-        B, P, i, pi, [&](uint32_t j) { return VR{__ldg(B.vel_b + j), __ldg(B.rho + j)}; },
-        [&](uint32_t, f3 rv, float, float4, VR d) {
+        B, P, i, pi, [&](uint32_t j) { return __ldg(B.vel_b + j); },
+        [&](uint32_t, f3 rv, float, float4, float4 vj) {
             float r2 = dot(rv, rv);
             float r = sqrtf(r2);
             float w = kernel_w(r, h);
-            f3 vd = sub(xyz(d.v), vi);
-            sum = add(sum, scale_r(scale(m / d.rho, vd), w));
+            f3 vd = sub(xyz(vj), vi);
+            sum = add(sum, scale_r(scale(m / vj.w, vd), w));
         });
     f3 vv = add(vi, scale(P.visc, sum));
     f3 g = {P.gx, P.gy, P.gz};
@@ -721,8 +722,9 @@ __device__ __forceinline__ void divergence_integration_body(const Bufs& B, int f
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     float4* vel = fixed ? B.vel_b : B.vel_a;
-    f3 nv = add(xyz(vel[i]), scale_r(xyz(*accp(B, i)), P.dt));
-    vel[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+    const float4 v0 = vel[i];
+    f3 nv = add(xyz(v0), scale_r(xyz(*accp(B, i)), P.dt));
+    vel[i] = make_float4(nv.x, nv.y, nv.z, v0.w);  // velocity_b.w keeps the density
     if (kLearn) after_solve_particle(B, L, P, i, 1);
 }
 
