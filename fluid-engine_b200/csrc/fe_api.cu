@@ -587,7 +587,7 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
         case FE_FIELD_POSITION_A: *dptr = c->B.pos_a; *elem = 16; break;
         case FE_FIELD_POSITION_B: *dptr = c->B.pos_b; *elem = 16; break;
         case FE_FIELD_VELOCITY_A: *dptr = c->B.vel_a; *elem = 16; break;
-        case FE_FIELD_VELOCITY_B: *dptr = c->B.vel_b; *elem = 16; break;
+        case FE_FIELD_VELOCITY_B: *dptr = c->B.pv + 1; *elem = 16; *pitch = 32; break;
         case FE_FIELD_DENSITY: *dptr = c->B.rho; *elem = 4; break;
         case FE_FIELD_FACTOR: *dptr = c->B.alpha; *elem = 4; break;
         case FE_FIELD_SOURCE_TERM: *dptr = c->B.src; *elem = 4; break;
@@ -891,7 +891,7 @@ fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n
     const size_t scratch_words = radix_scratch_words_any(n, c->key_bits);
     if ((s = dev_alloc(c, &B.pos_a, n)) || (s = dev_alloc(c, &B.pos_b, n)) ||
         (s = dev_alloc(c, &B.rec, 2 * (size_t)n)) ||
-        (s = dev_alloc(c, &B.vel_a, n)) || (s = dev_alloc(c, &B.vel_b, n)) ||
+        (s = dev_alloc(c, &B.vel_a, n)) || (s = dev_alloc(c, &B.pv, 2 * (size_t)n)) ||
         (s = dev_alloc(c, &B.rho, n)) ||
         (s = dev_alloc(c, &B.alpha, n)) || (s = dev_alloc(c, &B.src, n)) ||
         (s = dev_alloc(c, &B.prs, n)) || (s = dev_alloc(c, &B.prs_tmp, n)) ||
@@ -924,7 +924,7 @@ fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n
         FE_CUDA(cudaMemcpy(chunks_d, hc.data(), sizeof(uint4) * nchunks, cudaMemcpyHostToDevice));
         FE_CUDA(cudaMemset(B.rec, 0, (size_t)n * 32));
         FE_CUDA(cudaMemset(B.pos_b, 0, (size_t)n * 16));
-        FE_CUDA(cudaMemset(B.vel_b, 0, (size_t)n * 16));
+        FE_CUDA(cudaMemset(B.pv, 0, (size_t)n * 32));
         for (void* p : {(void*)B.rho, (void*)B.alpha, (void*)B.src, (void*)B.prs,
                         (void*)B.prs_tmp, (void*)B.nbr_count})
             FE_CUDA(cudaMemset(p, 0, (size_t)n * 4));
@@ -1121,9 +1121,12 @@ fe_status fe_upload(fe_ctx* c, fe_field f, const void* src, size_t bytes) {
     FE_CUDA(cudaSetDevice(c->device));
     FE_CUDA(cudaMemcpy2DAsync(d, pitch, src, elem, elem, need / elem, cudaMemcpyHostToDevice,
                               c->stream));
-    if (f == FE_FIELD_POSITION_B)  // keep pressure_update's copy in the records
+    if (f == FE_FIELD_POSITION_B) {  // keep the records' position copies
         FE_CUDA(cudaMemcpy2DAsync(c->B.rec, 32, src, 16, 16, c->n, cudaMemcpyHostToDevice,
                                   c->stream));
+        FE_CUDA(cudaMemcpy2DAsync(c->B.pv, 32, src, 16, 16, c->n, cudaMemcpyHostToDevice,
+                                  c->stream));
+    }
     // pos_b.w caches p / rho^2 for pressure_force, velocity_b.w rho for
     // viscosity.
     if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY || f == FE_FIELD_POSITION_B ||
@@ -1848,7 +1851,7 @@ std::vector<Section> state_sections(const fe_ctx* c, bool carry) {
                               {B.pos_a, n * 16},
                               {B.vel_a, n * 16},
                               {B.pos_b, n * 16},
-                              {B.vel_b, n * 16},
+                              {B.pv, n * 32},
                               {B.rec, n * 32},
                               {B.rho, n * 4},
                               {B.alpha, n * 4},

@@ -110,6 +110,28 @@ __device__ __forceinline__ float4* rec_pos(const Bufs& B, uint32_t i) {
 __device__ __forceinline__ float4* accp(const Bufs& B, uint32_t i) {
     return B.rec + 2 * (size_t)i + 1;
 }
+// velocity_b of particle i (second half of its position/velocity record).
+__device__ __forceinline__ float4* velb(const Bufs& B, uint32_t i) {
+    return B.pv + 2 * (size_t)i + 1;
+}
+
+// Both halves of record i of a 32-byte record array in one 256-bit store.
+__device__ __forceinline__ void st_pair(float4* base, uint32_t i, float4 a, float4 b) {
+    float4* p = base + 2 * (size_t)i;
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x),
+                 "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+                 : "memory");
+}
+
+// Both halves of record j of a 32-byte record array in one 256-bit
+// read-only load.
+__device__ __forceinline__ void ld_pair(const float4* base, uint32_t j, float4& a, float4& b) {
+    const float4* p = base + 2 * (size_t)j;
+    asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z),
+                   "=f"(b.w)
+                 : "l"(p));
+}
 
 // Both halves of particle i's record in one 256-bit store: the 32-byte sector
 // is written whole, so L2 never merges a half-written sector with DRAM.

@@ -74,9 +74,13 @@ enum Ticket : int { kTicketStats = 0, kTicketSolve = 1, kTicketHist = 2 };
 
 // Kernel-side view of every buffer of a context (passed by value).
 struct Bufs {
-    // velocity_b.w holds the slot's density (written by density_alpha, kept by
-    // the FIXED-mode divergence integration) for viscosity's gathers.
-    float4 *pos_a, *vel_a, *vel_b;
+    float4 *pos_a, *vel_a;
+    // 32-byte record per particle: pv[2i] = copy of position_b (xyz, written
+    // by reorder), pv[2i+1] = velocity_b with the slot's density in w
+    // (written by density_alpha, kept by the FIXED-mode divergence
+    // integration).  Viscosity and the FIXED-mode divergence source fetch a
+    // neighbour's position, velocity and density with one 256-bit load.
+    float4* pv;
     // position_b; w holds p / rho^2 (NaN when rho <= 1e-6) for pressure_force.
     float4* pos_b;
     // 32-byte record per particle: rec[2i] = copy of position_b (xyz),

@@ -84,7 +84,7 @@ __device__ __forceinline__ void reorder_body(const Bufs& B, int carry_pressure,
     float4 p = __ldg(B.pos_a + src);
     p.w = pressure_over_rho2(B.prs[i], B.rho[i]);
     *posb(B, i) = p;
-    B.vel_b[i] = __ldg(B.vel_a + src);
+    st_pair(B.pv, i, p, __ldg(B.vel_a + src));   // position copy, velocity_b
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
     if (kCarry) L.carry_tmp[i] = L.carry[src];
 }
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
     posb(B, i)->w = pressure_over_rho2(B.prs[i], B.rho[i]);
-    B.vel_b[i].w = B.rho[i];
+    velb(B, i)->w = B.rho[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
     }
     B.rho[i] = a.density;
     // velocity_b.w carries the density for viscosity's neighbour gathers
-    B.vel_b[i].w = a.density;
+    velb(B, i)->w = a.density;
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
     B.alpha[i] = al > kEpsR ? al : 0.0f;
     B.nbr_count[i] = a.cnt;
@@ -364,12 +364,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
     const f3 pi = xyz(__ldg(posb(B, i)));
-    const f3 vi = xyz(__ldg(B.vel_b + i));
+    const f3 vi = xyz(__ldg(velb(B, i)));
     f3 sum = {0.0f, 0.0f, 0.0f};
-    // velocity_b.w = rho_j (written by density_alpha): one gather per neighbour
-    for_each_neighbor(
-        B, P, i, pi, [&](uint32_t j) { return __ldg(B.vel_b + j); },
-        [&](uint32_t, f3 rv, float, float4, float4 vj) {
+    // velocity_b.w = rho_j (written by density_alpha): one 256-bit load of the
+    // position/velocity record per neighbour
+    for_each_neighbor_pair(
+        B, P, i, pi, B.pv, [&](f3 rv, float, float4 vj) {
             float r2 = dot(rv, rv);
             float r = sqrtf(r2);
             float w = kernel_w(r, h);
@@ -437,20 +437,28 @@ __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
     const float m = P.mass;
-    const float4* __restrict__ vel = fixed ? B.vel_b : B.vel_a;
     const f3 pi = xyz(__ldg(posb(B, i)));
-    const f3 vi = xyz(__ldg(vel + i));
+    const f3 vi = xyz(__ldg(fixed ? velb(B, i) : B.vel_a + i));
     float div = 0.0f;
     Moments mo;
-    for_each_neighbor(
-        B, P, i, pi,
-        [&](uint32_t j) { return VelRho{__ldg(vel + j), kLearn ? __ldg(B.rho + j) : 0.0f}; },
-        [&](uint32_t, f3 rv, float g, float4, VelRho d) {
-            f3 grad = scale(g, rv);
-            f3 vd = sub(vi, xyz(d.v));
-            div += m * dot(vd, grad);
-            if (kLearn) mo.add(g, d.rho, P.rho0);
-        });
+    auto term = [&](f3 rv, float g, float4 vj, float rho_j) {
+        f3 grad = scale(g, rv);
+        f3 vd = sub(vi, xyz(vj));
+        div += m * dot(vd, grad);
+        if (kLearn) mo.add(g, rho_j, P.rho0);
+    };
+    if (fixed) {
+        // velocity_b and its density from the position/velocity record
+        for_each_neighbor_pair(B, P, i, pi, B.pv,
+                               [&](f3 rv, float g, float4 vj) { term(rv, g, vj, vj.w); });
+    } else {
+        for_each_neighbor(
+            B, P, i, pi,
+            [&](uint32_t j) {
+                return VelRho{__ldg(B.vel_a + j), kLearn ? __ldg(B.rho + j) : 0.0f};
+            },
+            [&](uint32_t, f3 rv, float g, float4, VelRho d) { term(rv, g, d.v, d.rho); });
+    }
     B.src[i] = -div;
     if (kLearn) emit_features(B, L, P, i, s, 1, -div, div, vi, mo);
 }
@@ -721,10 +729,10 @@ __device__ __forceinline__ void divergence_integration_body(const Bufs& B, int f
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
-    float4* vel = fixed ? B.vel_b : B.vel_a;
-    const float4 v0 = vel[i];
+    float4* vel = fixed ? velb(B, i) : B.vel_a + i;
+    const float4 v0 = *vel;
     f3 nv = add(xyz(v0), scale_r(xyz(*accp(B, i)), P.dt));
-    vel[i] = make_float4(nv.x, nv.y, nv.z, v0.w);  // velocity_b.w keeps the density
+    *vel = make_float4(nv.x, nv.y, nv.z, v0.w);  // velocity_b.w keeps the density
     if (kLearn) after_solve_particle(B, L, P, i, 1);
 }
 
@@ -753,11 +761,12 @@ __global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upar
     uint32_t i, s, c;
     bool valid = chunk_of(B, i, s, c);
     const DevParams& P = B.P[s];
-    const float4* vel = fixed ? B.vel_b : B.vel_a;
+    const float4* vel = fixed ? velb(B, 0) : B.vel_a;
+    const uint32_t vstride = fixed ? 2u : 1u;
     uint32_t mx = 0, s1 = 0, s2 = 0, bad = 0;
     double d1 = 0.0, d2 = 0.0;
     if (valid) {
-        float4 v = vel[i];
+        float4 v = vel[(size_t)i * vstride];
         float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
         mx = __float_as_uint(speed);
         float rho = B.rho[i], src = B.src[i];

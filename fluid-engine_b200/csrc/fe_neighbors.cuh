@@ -104,11 +104,15 @@ __device__ __forceinline__ void for_each_neighbor(const Bufs& B, const DevParams
 
 struct NoData {};
 
-// As for_each_neighbor, for pressure_update: f(r_vec, grad_scale, acc_j),
-// with position and acceleration of j fetched by one 256-bit load.
+// As for_each_neighbor, over a 32-byte record array whose first half of
+// record j is a copy of position_b: f(r_vec, grad_scale, second_half_j), with
+// both halves of j fetched by one 256-bit load.  B.rec (position,
+// acceleration) for pressure_update, B.pv (position, velocity_b) for
+// viscosity and the FIXED-mode divergence source.
 template <class F>
-__device__ __forceinline__ void for_each_neighbor_record(const Bufs& B, const DevParams& P,
-                                                         uint32_t i, f3 pi, F&& f) {
+__device__ __forceinline__ void for_each_neighbor_pair(const Bufs& B, const DevParams& P,
+                                                       uint32_t i, f3 pi, const float4* recs,
+                                                       F&& f) {
     const uint32_t cnt = B.nbr_count[i];
     if (cnt <= kNbrCap) {
         const uint2* e = B.nbr + i;
@@ -121,10 +125,10 @@ __device__ __forceinline__ void for_each_neighbor_record(const Bufs& B, const De
             uint2 v2 = ld_list(e + (k + 2) * stride, pol);
             uint2 v3 = ld_list(e + (k + 3) * stride, pol);
             float4 q0, a0, q1, a1, q2, a2, q3, a3;
-            ld_record(B, v0.x, q0, a0);
-            ld_record(B, v1.x, q1, a1);
-            ld_record(B, v2.x, q2, a2);
-            ld_record(B, v3.x, q3, a3);
+            ld_pair(recs, v0.x, q0, a0);
+            ld_pair(recs, v1.x, q1, a1);
+            ld_pair(recs, v2.x, q2, a2);
+            ld_pair(recs, v3.x, q3, a3);
             f(sub(pi, xyz(q0)), __uint_as_float(v0.y), a0);
             f(sub(pi, xyz(q1)), __uint_as_float(v1.y), a1);
             f(sub(pi, xyz(q2)), __uint_as_float(v2.y), a2);
@@ -133,16 +137,22 @@ __device__ __forceinline__ void for_each_neighbor_record(const Bufs& B, const De
         for (; k < cnt; ++k) {
             uint2 v = ld_list(e + k * stride, pol);
             float4 q, a;
-            ld_record(B, v.x, q, a);
+            ld_pair(recs, v.x, q, a);
             f(sub(pi, xyz(q)), __uint_as_float(v.y), a);
         }
     } else {
         const float h = P.h;
         walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
             float r = sqrtf(r2);
-            if (r > kEpsR) f(rv, kernel_grad_scale(r, h), __ldg(accp(B, j)));
+            if (r > kEpsR) f(rv, kernel_grad_scale(r, h), __ldg(recs + 2 * (size_t)j + 1));
         });
     }
+}
+
+template <class F>
+__device__ __forceinline__ void for_each_neighbor_record(const Bufs& B, const DevParams& P,
+                                                         uint32_t i, f3 pi, F&& f) {
+    for_each_neighbor_pair(B, P, i, pi, B.rec, f);
 }
 
 }  // namespace fe
