@@ -586,7 +586,7 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
     switch (f) {
         case FE_FIELD_POSITION_A: *dptr = c->B.pos_a; *elem = 16; break;
         case FE_FIELD_POSITION_B: *dptr = c->B.pos_b; *elem = 16; break;
-        case FE_FIELD_VELOCITY_A: *dptr = c->B.vel_a; *elem = 16; break;
+        case FE_FIELD_VELOCITY_A: *dptr = c->B.pa + 1; *elem = 16; *pitch = 32; break;
         case FE_FIELD_VELOCITY_B: *dptr = c->B.pv + 1; *elem = 16; *pitch = 32; break;
         case FE_FIELD_DENSITY: *dptr = c->B.rho; *elem = 4; break;
         case FE_FIELD_FACTOR: *dptr = c->B.alpha; *elem = 4; break;
@@ -891,7 +891,7 @@ fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n
     const size_t scratch_words = radix_scratch_words_any(n, c->key_bits);
     if ((s = dev_alloc(c, &B.pos_a, n)) || (s = dev_alloc(c, &B.pos_b, n)) ||
         (s = dev_alloc(c, &B.rec, 2 * (size_t)n)) ||
-        (s = dev_alloc(c, &B.vel_a, n)) || (s = dev_alloc(c, &B.pv, 2 * (size_t)n)) ||
+        (s = dev_alloc(c, &B.pa, 2 * (size_t)n)) || (s = dev_alloc(c, &B.pv, 2 * (size_t)n)) ||
         (s = dev_alloc(c, &B.rho, n)) ||
         (s = dev_alloc(c, &B.alpha, n)) || (s = dev_alloc(c, &B.src, n)) ||
         (s = dev_alloc(c, &B.prs, n)) || (s = dev_alloc(c, &B.prs_tmp, n)) ||
@@ -920,7 +920,8 @@ fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n
         for (uint32_t i = 0; i < n; ++i)
             h4[i] = vel_xyz ? make_float4(vel_xyz[3 * i], vel_xyz[3 * i + 1], vel_xyz[3 * i + 2], 0.0f)
                             : make_float4(0, 0, 0, 0);
-        FE_CUDA(cudaMemcpy(B.vel_a, h4.data(), (size_t)n * 16, cudaMemcpyHostToDevice));
+        FE_CUDA(cudaMemset(B.pa, 0, (size_t)n * 32));
+        FE_CUDA(cudaMemcpy2D(B.pa + 1, 32, h4.data(), 16, 16, n, cudaMemcpyHostToDevice));
         FE_CUDA(cudaMemcpy(chunks_d, hc.data(), sizeof(uint4) * nchunks, cudaMemcpyHostToDevice));
         FE_CUDA(cudaMemset(B.rec, 0, (size_t)n * 32));
         FE_CUDA(cudaMemset(B.pos_b, 0, (size_t)n * 16));
@@ -1126,11 +1127,12 @@ fe_status fe_upload(fe_ctx* c, fe_field f, const void* src, size_t bytes) {
                                   c->stream));
         FE_CUDA(cudaMemcpy2DAsync(c->B.pv, 32, src, 16, 16, c->n, cudaMemcpyHostToDevice,
                                   c->stream));
+        FE_CUDA(cudaMemcpy2DAsync(c->B.pa, 32, src, 16, 16, c->n, cudaMemcpyHostToDevice,
+                                  c->stream));
     }
-    // pos_b.w caches p / rho^2 for pressure_force, velocity_b.w rho for
-    // viscosity.
+    // pos_b.w caches p / rho^2 for pressure_force, the velocities' w rho.
     if (f == FE_FIELD_PRESSURE || f == FE_FIELD_DENSITY || f == FE_FIELD_POSITION_B ||
-        f == FE_FIELD_VELOCITY_B)
+        f == FE_FIELD_VELOCITY_A || f == FE_FIELD_VELOCITY_B)
         return run_refresh_pr(c);
     return FE_OK;
 }
@@ -1160,9 +1162,9 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
         float* v = static_cast<float*>(dst);
         for (uint32_t i = 0; i < c->n; ++i) v[4 * i + 3] = 1.0f;
     }
-    if (f == FE_FIELD_VELOCITY_B) {
-        // The device keeps the density in w; the reference's velocity_b.w is
-        // the copied velocity_a.w, which its passes always write as 0.
+    if (f == FE_FIELD_VELOCITY_A || f == FE_FIELD_VELOCITY_B) {
+        // The device keeps the density in w; the reference's passes always
+        // write the velocities' w as 0.
         float* v = static_cast<float*>(dst);
         for (uint32_t i = 0; i < c->n; ++i) v[4 * i + 3] = 0.0f;
     }
@@ -1849,7 +1851,7 @@ std::vector<Section> state_sections(const fe_ctx* c, bool carry) {
                               {B.S, sizeof(SceneState) * ns},
                               {B.G, sizeof(GlobalState)},
                               {B.pos_a, n * 16},
-                              {B.vel_a, n * 16},
+                              {B.pa, n * 32},
                               {B.pos_b, n * 16},
                               {B.pv, n * 32},
                               {B.rec, n * 32},

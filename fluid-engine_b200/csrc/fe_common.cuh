@@ -110,6 +110,10 @@ __device__ __forceinline__ float4* rec_pos(const Bufs& B, uint32_t i) {
 __device__ __forceinline__ float4* accp(const Bufs& B, uint32_t i) {
     return B.rec + 2 * (size_t)i + 1;
 }
+// velocity_a of particle i (second half of its position/velocity record).
+__device__ __forceinline__ float4* vela(const Bufs& B, uint32_t i) {
+    return B.pa + 2 * (size_t)i + 1;
+}
 // velocity_b of particle i (second half of its position/velocity record).
 __device__ __forceinline__ float4* velb(const Bufs& B, uint32_t i) {
     return B.pv + 2 * (size_t)i + 1;

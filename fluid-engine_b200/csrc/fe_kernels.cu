@@ -84,7 +84,11 @@ __device__ __forceinline__ void reorder_body(const Bufs& B, int carry_pressure,
     float4 p = __ldg(B.pos_a + src);
     p.w = pressure_over_rho2(B.prs[i], B.rho[i]);
     *posb(B, i) = p;
-    st_pair(B.pv, i, p, __ldg(B.vel_a + src));   // position copy, velocity_b
+    // position copy + velocity_b; then this slot's velocity_a record with the
+    // new position copy (its velocity half is rewritten unchanged, so the
+    // gathers of other threads read the same bytes either way)
+    st_pair(B.pv, i, p, *vela(B, src));
+    st_pair(B.pa, i, p, *vela(B, i));
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
     if (kCarry) L.carry_tmp[i] = L.carry[src];
 }
@@ -124,6 +128,7 @@ __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     if (i >= B.n_total) return;
     posb(B, i)->w = pressure_over_rho2(B.prs[i], B.rho[i]);
     velb(B, i)->w = B.rho[i];
+    vela(B, i)->w = B.rho[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -379,7 +384,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
     f3 vv = add(vi, scale(P.visc, sum));
     f3 g = {P.gx, P.gy, P.gz};
     f3 vf = add(vv, scale_r(g, P.dt));
-    B.vel_a[i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
+    // the whole position/velocity_a record; w = the slot's density for the
+    // learned density source
+    st_pair(B.pa, i, make_float4(pi.x, pi.y, pi.z, 0.0f),
+            make_float4(vf.x, vf.y, vf.z, B.rho[i]));
 }
 
 // ---------------------------------------------------------------------------
@@ -398,18 +406,16 @@ __device__ __forceinline__ void density_source_body(const Bufs& B, const LearnAr
     const DevParams& P = B.P[s];
     const float m = P.mass, dt = P.dt;
     const f3 pi = xyz(__ldg(posb(B, i)));
-    const f3 vi = xyz(__ldg(B.vel_a + i));
+    const f3 vi = xyz(__ldg(vela(B, i)));
     float div = 0.0f;
     Moments mo;
-    for_each_neighbor(
-        B, P, i, pi,
-        [&](uint32_t j) { return VelRho{__ldg(B.vel_a + j), kLearn ? __ldg(B.rho + j) : 0.0f}; },
-        [&](uint32_t, f3 rv, float g, float4, VelRho d) {
-            f3 grad = scale(g, rv);
-            f3 vd = sub(vi, xyz(d.v));
-            div += m * dot(vd, grad);
-            if (kLearn) mo.add(g, d.rho, P.rho0);
-        });
+    // velocity_a and (w) the density of j from one load of its record
+    for_each_neighbor_pair(B, P, i, pi, B.pa, [&](f3 rv, float g, float4 vj) {
+        f3 grad = scale(g, rv);
+        f3 vd = sub(vi, xyz(vj));
+        div += m * dot(vd, grad);
+        if (kLearn) mo.add(g, vj.w, P.rho0);
+    });
     float rho_i = B.rho[i];
     float source = 0.0f;
     if (dt > kEpsR) source = ((P.rho0 - rho_i) / dt) - div;
@@ -438,7 +444,7 @@ __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
     const DevParams& P = B.P[s];
     const float m = P.mass;
     const f3 pi = xyz(__ldg(posb(B, i)));
-    const f3 vi = xyz(__ldg(fixed ? velb(B, i) : B.vel_a + i));
+    const f3 vi = xyz(__ldg(fixed ? velb(B, i) : vela(B, i)));
     float div = 0.0f;
     Moments mo;
     auto term = [&](f3 rv, float g, float4 vj, float rho_j) {
@@ -455,7 +461,7 @@ __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
         for_each_neighbor(
             B, P, i, pi,
             [&](uint32_t j) {
-                return VelRho{__ldg(B.vel_a + j), kLearn ? __ldg(B.rho + j) : 0.0f};
+                return VelRho{__ldg(vela(B, j)), kLearn ? __ldg(B.rho + j) : 0.0f};
             },
             [&](uint32_t, f3 rv, float g, float4, VelRho d) { term(rv, g, d.v, d.rho); });
     }
@@ -690,7 +696,8 @@ __device__ __forceinline__ void pressure_integration_body(const Bufs& B, const L
     const float dt = P.dt, r = P.radius;
     const float rest = 0.5f, fric = 0.95f, eps = 0.001f;
     f3 pos = xyz(__ldg(posb(B, i)));
-    f3 vel = xyz(B.vel_a[i]);
+    const float4 v0 = *vela(B, i);
+    f3 vel = xyz(v0);
     f3 ap = xyz(*accp(B, i));
     f3 nv = add(vel, scale_r(ap, dt));
     f3 np = add(pos, scale_r(nv, dt));
@@ -710,7 +717,7 @@ __device__ __forceinline__ void pressure_integration_body(const Bufs& B, const L
         np.z = P.bmaxz - r - eps; nv.z *= -rest; nv.x *= fric; nv.y *= fric;
     }
     B.pos_a[i] = make_float4(np.x, np.y, np.z, 1.0f);
-    B.vel_a[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+    *vela(B, i) = make_float4(nv.x, nv.y, nv.z, v0.w);
     if (kLearn) after_solve_particle(B, L, P, i, 0);
 }
 
@@ -729,7 +736,7 @@ __device__ __forceinline__ void divergence_integration_body(const Bufs& B, int f
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     const DevParams& P = B.P[s];
-    float4* vel = fixed ? velb(B, i) : B.vel_a + i;
+    float4* vel = fixed ? velb(B, i) : vela(B, i);
     const float4 v0 = *vel;
     f3 nv = add(xyz(v0), scale_r(xyz(*accp(B, i)), P.dt));
     *vel = make_float4(nv.x, nv.y, nv.z, v0.w);  // velocity_b.w keeps the density
@@ -761,8 +768,8 @@ __global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upar
     uint32_t i, s, c;
     bool valid = chunk_of(B, i, s, c);
     const DevParams& P = B.P[s];
-    const float4* vel = fixed ? velb(B, 0) : B.vel_a;
-    const uint32_t vstride = fixed ? 2u : 1u;
+    const float4* vel = fixed ? velb(B, 0) : vela(B, 0);
+    const uint32_t vstride = 2u;
     uint32_t mx = 0, s1 = 0, s2 = 0, bad = 0;
     double d1 = 0.0, d2 = 0.0;
     if (valid) {

@@ -13,7 +13,7 @@ from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
                     c_int32, c_size_t, c_uint32, c_uint64, c_void_p)
 
 ABI_VERSION = 1
-FE_STATE_VERSION = 2
+FE_STATE_VERSION = 3
 
 # fe_status
 FE_OK = 0

@@ -376,7 +376,7 @@ FE_API fe_status fe_read_scene_stats(fe_ctx* ctx, uint32_t scene, fe_stats* out)
  *   table size and scene layout (FE_ERR_INVALID_ARGUMENT otherwise, and for a
  *   damaged header or a short buffer; the context is then unchanged).
  *   Recorded frame graphs are dropped.  An attached model stays attached. */
-#define FE_STATE_VERSION 2u
+#define FE_STATE_VERSION 3u
 FE_API fe_status fe_state_size(const fe_ctx* ctx, size_t* bytes);
 FE_API fe_status fe_state_export(fe_ctx* ctx, void* dst, size_t bytes);
 FE_API fe_status fe_state_import(fe_ctx* ctx, const void* src, size_t bytes);
