@@ -514,7 +514,9 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
         return s;
     if ((s = rec_neighbor_search(c, R))) return s;
     if ((s = rec_simple(c, R, k_density_alpha))) return s;
-    if (c->carries())
+    if (c->carries() && fixed)
+        REC(R.k(k_divergence_source_learn_fixed, chunk_grid(c), dim3(kBlock), B, c->L));
+    else if (c->carries())
         REC(R.k(k_divergence_source_learn, chunk_grid(c), dim3(kBlock), B, fixed, c->L));
     else
         REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));

@@ -472,6 +472,11 @@ __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
 __global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fixed) {
     divergence_source_body<false>(B, fixed, LearnArgs{});
 }
+// FIXED mode with the learned state: the mode is a constant, so only the
+// record path is compiled (fewer registers, four blocks per SM).
+__global__ void __launch_bounds__(kBlock, 4) k_divergence_source_learn_fixed(Bufs B, LearnArgs L) {
+    divergence_source_body<true>(B, 1, L);
+}
 __global__ void __launch_bounds__(kBlock, 3) k_divergence_source_learn(Bufs B, int fixed,
                                                                         LearnArgs L) {
     divergence_source_body<true>(B, fixed, L);

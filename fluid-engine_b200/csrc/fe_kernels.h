@@ -38,6 +38,7 @@ __global__ void k_frame_prologue(Bufs B);
 __global__ void k_count_substep(Bufs B);
 __global__ void k_density_source_learn(Bufs B, LearnArgs L);
 __global__ void k_divergence_source_learn(Bufs B, int fixed, LearnArgs L);
+__global__ void k_divergence_source_learn_fixed(Bufs B, LearnArgs L);
 __global__ void k_warm_apply(Bufs B, LearnArgs L, int which);
 __global__ void k_carry_take(Bufs B, LearnArgs L);
 
