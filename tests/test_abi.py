@@ -156,3 +156,15 @@ def test_debug_hooks_validate_before_device_work(lib):
     assert lib.fe_debug_bounded_wait(0, 10, None) == _abi.FE_ERR_INVALID_ARGUMENT
     lib.fe_debug_fail_allocation(0)
     lib.fe_debug_poison_allocations(0)
+
+
+def test_header_constants_match_the_python_mirror():
+    text = open(HEADER).read()
+    for name, value in [("FE_STATE_VERSION", _abi.FE_STATE_VERSION),
+                        ("FE_ABI_VERSION", _abi.ABI_VERSION),
+                        ("FE_MAX_PARTICLES", None)]:
+        m = re.search(rf"#define {name} \(?([0-9]+)u?(?: << ([0-9]+))?\)?", text)
+        assert m, name
+        v = int(m.group(1)) << int(m.group(2) or 0)
+        if value is not None:
+            assert v == value, (name, v, value)
