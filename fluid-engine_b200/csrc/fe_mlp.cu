@@ -136,11 +136,9 @@ __device__ __forceinline__ float tanh_hw(float x) {
 
 // SiLU z * sigmoid(z) with sigmoid(z) = (1 + tanh(z / 2)) / 2, i.e.
 // s + s * tanh(s) for s = z / 2: one special-function op per activation
-// instead of an exponential and a reciprocal.
-__device__ __forceinline__ float silu(float z) {
-    const float s = 0.5f * z;
-    return s + s * tanh_hw(s);
-}
+// instead of an exponential and a reciprocal, and one fused multiply-add.
+__device__ __forceinline__ float silu_half(float s) { return __fmaf_rn(s, tanh_hw(s), s); }
+__device__ __forceinline__ float silu(float z) { return silu_half(0.5f * z); }
 __device__ __forceinline__ float silu_grad(float z) {
     const float sg = 0.5f + 0.5f * tanh_hw(0.5f * z);
     return sg * (1.0f + z * (1.0f - sg));
@@ -257,8 +255,11 @@ __device__ __forceinline__ void epilogue_half(uint32_t taddr, uint32_t c0, const
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const uint32_t c = c0 + cc + g + 2 * j;
-                __nv_bfloat162 two = __floats2bfloat162_rn(silu(v[g + 2 * j] + bias[c]),
-                                                           silu(v[g + 2 * j + 1] + bias[c + 1]));
+                // bias holds b / 2: fma(v, 1/2, b / 2) = (v + b) / 2 exactly as
+                // the training kernel's 0.5f * (v + b) (halving is exact)
+                __nv_bfloat162 two = __floats2bfloat162_rn(
+                    silu_half(__fmaf_rn(v[g + 2 * j], 0.5f, bias[c])),
+                    silu_half(__fmaf_rn(v[g + 2 * j + 1], 0.5f, bias[c + 1])));
                 w[j] = *reinterpret_cast<uint32_t*>(&two);
             }
             *reinterpret_cast<uint4*>(out + off_k(row, c0 + cc + g, 64)) =
@@ -286,9 +287,9 @@ __global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
         *reinterpret_cast<__nv_bfloat16*>(S.W.w3 + off_k(o, k, 64)) =
             o < 2 ? P.w3[o * 64 + k] : __float2bfloat16_rn(0.0f);
     }
-    if (tid < 64) {
-        S.W.b1[tid] = P.b1[tid];
-        S.W.b2[tid] = P.b2[tid];
+    if (tid < 64) {  // hidden-layer biases halved for the epilogue's fused SiLU
+        S.W.b1[tid] = 0.5f * P.b1[tid];
+        S.W.b2[tid] = 0.5f * P.b2[tid];
     }
     if (tid < 16) S.W.b3[tid] = tid < 2 ? P.b3[tid] : 0.0f;
     if (tid == 0) bar_init(&S.bar);
