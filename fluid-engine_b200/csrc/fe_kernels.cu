@@ -121,8 +121,8 @@ __global__ void __launch_bounds__(kBlock) k_take_pressure_carry(Bufs B, LearnArg
     take_pressure_body<true>(B, L);
 }
 
-// pr = p / rho^2 and velocity_b.w = rho for all particles (after a host
-// upload of p, rho, position_b or velocity_b).
+// pr = p / rho^2 and both velocities' w = rho for all particles (after a
+// host upload of p, rho, position_b or a velocity).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
@@ -351,7 +351,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
         });
     }
     B.rho[i] = a.density;
-    // velocity_b.w carries the density for viscosity's neighbour gathers
+    // velocity_b.w carries the density for the neighbour gathers of viscosity
+    // and the FIXED-mode divergence source
     velb(B, i)->w = a.density;
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
     B.alpha[i] = al > kEpsR ? al : 0.0f;
@@ -744,7 +745,7 @@ __device__ __forceinline__ void divergence_integration_body(const Bufs& B, int f
     float4* vel = fixed ? velb(B, i) : vela(B, i);
     const float4 v0 = *vel;
     f3 nv = add(xyz(v0), scale_r(xyz(*accp(B, i)), P.dt));
-    *vel = make_float4(nv.x, nv.y, nv.z, v0.w);  // velocity_b.w keeps the density
+    *vel = make_float4(nv.x, nv.y, nv.z, v0.w);  // w (the density) is kept
     if (kLearn) after_solve_particle(B, L, P, i, 1);
 }
 
