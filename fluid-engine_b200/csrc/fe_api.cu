@@ -430,10 +430,13 @@ fe_status rec_simple(fe_ctx* c, Recorder& R, void (*kern)(Bufs)) {
 
 fe_status rec_stats(fe_ctx* c, Recorder& R) {
     REC(R.k(k_stats, chunk_grid(c), dim3(kBlock), c->B, c->fixed_mode() ? 1 : 0, c->upart));
+    if (c->B.n_scenes > 1)  // the per-scene finish, one block per scene
+        REC(R.k(k_stats_finish, dim3(c->B.n_scenes), dim3(kBlock), c->B, c->upart));
     return FE_OK;
 }
 
-// One Jacobi solve.  Graph: begin kernel, WHILE node {force, update}, end
+// One Jacobi solve.  Graph: begin kernel, WHILE node {force, update, the
+// per-scene finish when the context holds several scenes, guard}, end
 // kernel.  Eager: the same kernels with a host loop on the device flag.
 fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
     Bufs B = c->B;
@@ -448,6 +451,9 @@ fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
             REC(R.k(k_pressure_force, chunk_grid(c), dim3(kBlock), B, which));
             REC(R.k(k_pressure_update, chunk_grid(c), dim3(kBlock), B, which,
                     (cudaGraphConditionalHandle)0, 0));
+            if (B.n_scenes > 1)
+                REC(R.k(k_solve_finish, dim3(B.n_scenes), dim3(kBlock), B, which,
+                        (cudaGraphConditionalHandle)0, 0));
         }
         REC(R.k(k_solve_end, dim3(1), dim3(32), B, which));
         return FE_OK;
@@ -471,6 +477,8 @@ fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
     body.root = R.root;
     REC(body.k(k_pressure_force, chunk_grid(c), dim3(kBlock), B, which));
     REC(body.k(k_pressure_update, chunk_grid(c), dim3(kBlock), B, which, h, 1));
+    if (B.n_scenes > 1)  // the per-scene finish, one block per scene
+        REC(body.k(k_solve_finish, dim3(B.n_scenes), dim3(kBlock), B, which, h, 1));
     REC(body.k(k_loop_guard, dim3(1), dim3(32), B, which, h));
     R.last = node;
     REC(R.k(k_solve_end, dim3(1), dim3(32), B, which));

@@ -528,51 +528,85 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which)
 // turns the per-scene sums into the metric, advances the iteration count and
 // sets the loop condition.
 // ---------------------------------------------------------------------------
-__device__ void solve_finish(Bufs& B, int which, cudaGraphConditionalHandle handle,
-                             int use_handle, double* smem) {
-    // Runs in the last block only: per scene, final sum and control update.
-    uint32_t any_open = 0;
-    uint32_t c0 = 0;
-    for (uint32_t s = 0; s < B.n_scenes; ++s) {
-        const DevParams& P = B.P[s];
-        SolveCtl& ctl = B.S[s].solve[which];
-        uint32_t nchunks = (P.n + kBlock - 1) / kBlock;
-        bool active = !ctl.done;
-        double sum = 0.0, mx = 0.0;
-        if (active && P.solver == 1u) {
-            sum = block_final_sum(B.partials + c0, nchunks, smem);
-            double m = 0.0;
-            for (uint32_t k = threadIdx.x; k < nchunks; k += kBlock)
-                m = fmax(m, __ldcg(B.partials + B.n_chunks + c0 + k));
-            mx = block_max256(m, smem);
-        }
-        if (threadIdx.x == 0 && active) {
-            ctl.iter += 1;
-            if (P.solver == 1u) {
-                double avg = sum / (double)P.n;
-                if (which == 1) avg = avg * (double)P.dt;
-                double metric = avg / (double)P.rho0;
-                double metric_max = (which == 1 ? mx * (double)P.dt : mx) / (double)P.rho0;
-                ctl.metric = metric;
-                ctl.metric_max = metric_max;
-                float tol = which == 0 ? P.tol_d : P.tol_v;
-                if (ctl.iter >= P.min_it && metric <= (double)tol) {
-                    ctl.done = 1;
-                } else if (ctl.iter >= P.max_it) {
-                    ctl.done = 1;
-                    ctl.cap_hit = 1;
-                }
-            } else {
-                if (ctl.iter >= ctl.K) ctl.done = 1;
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && !ctl.done) any_open = 1;
-        c0 += nchunks;
+// Index of scene sc's first chunk (chunks are laid out scene by scene): a
+// block-wide sum of the chunk counts of the scenes before it.  `tmp` holds 8
+// words.  Whole block.
+__device__ __forceinline__ uint32_t scene_chunk_base(const Bufs& B, uint32_t sc, uint32_t* tmp) {
+    uint32_t t = 0;
+    for (uint32_t k = threadIdx.x; k < sc; k += kBlock) t += (B.P[k].n + kBlock - 1) / kBlock;
+    for (int m = 16; m >= 1; m >>= 1) t += __shfl_xor_sync(kFull, t, m);
+    if (lane_id() == 0) tmp[threadIdx.x >> 5] = t;
+    __syncthreads();
+    uint32_t r = 0;
+    for (int w = 0; w < 8; ++w) r += tmp[w];
+    __syncthreads();
+    return r;
+}
+
+// Solver control of scene s after an iteration (whole block): the final
+// fixed-order sum of its chunk partials, the metric, iteration count and
+// done flag.  c0 = the scene's first chunk.
+__device__ void solve_finish_scene(Bufs& B, int which, uint32_t s, uint32_t c0, double* smem) {
+    const DevParams& P = B.P[s];
+    SolveCtl& ctl = B.S[s].solve[which];
+    uint32_t nchunks = (P.n + kBlock - 1) / kBlock;
+    bool active = !ctl.done;
+    double sum = 0.0, mx = 0.0;
+    if (active && P.solver == 1u) {
+        sum = block_final_sum(B.partials + c0, nchunks, smem);
+        double m = 0.0;
+        for (uint32_t k = threadIdx.x; k < nchunks; k += kBlock)
+            m = fmax(m, __ldcg(B.partials + B.n_chunks + c0 + k));
+        mx = block_max256(m, smem);
     }
-    if (threadIdx.x == 0) {
-        B.G->cond[which] = any_open;
-        if (use_handle) cudaGraphSetConditional(handle, any_open);
+    if (threadIdx.x == 0 && active) {
+        ctl.iter += 1;
+        if (P.solver == 1u) {
+            double avg = sum / (double)P.n;
+            if (which == 1) avg = avg * (double)P.dt;
+            double metric = avg / (double)P.rho0;
+            double metric_max = (which == 1 ? mx * (double)P.dt : mx) / (double)P.rho0;
+            ctl.metric = metric;
+            ctl.metric_max = metric_max;
+            float tol = which == 0 ? P.tol_d : P.tol_v;
+            if (ctl.iter >= P.min_it && metric <= (double)tol) {
+                ctl.done = 1;
+            } else if (ctl.iter >= P.max_it) {
+                ctl.done = 1;
+                ctl.cap_hit = 1;
+            }
+        } else {
+            if (ctl.iter >= ctl.K) ctl.done = 1;
+        }
+    }
+    __syncthreads();
+}
+
+// Sets the loop condition from every scene's done flag (thread 0).
+__device__ __forceinline__ void solve_set_condition(Bufs& B, int which,
+                                                    cudaGraphConditionalHandle handle,
+                                                    int use_handle) {
+    uint32_t any_open = 0;
+    for (uint32_t s = 0; s < B.n_scenes; ++s)
+        if (!__ldcg(&B.S[s].solve[which].done)) any_open = 1;
+    B.G->cond[which] = any_open;
+    if (use_handle) cudaGraphSetConditional(handle, any_open);
+}
+
+// Multi-scene contexts: the per-scene finish in parallel, one block per
+// scene (the same per-scene code, so the same sums); the last block sets the
+// loop condition.
+__global__ void __launch_bounds__(kBlock) k_solve_finish(Bufs B, int which,
+                                                         cudaGraphConditionalHandle handle,
+                                                         int use_handle) {
+    __shared__ double smem[8];
+    __shared__ uint32_t tmp[8];
+    const uint32_t s = blockIdx.x;
+    const uint32_t c0 = scene_chunk_base(B, s, tmp);
+    solve_finish_scene(B, which, s, c0, smem);
+    if (last_block_done(&B.G->tickets[kTicketSolve], gridDim.x) && threadIdx.x == 0) {
+        solve_set_condition(B, which, handle, use_handle);
+        B.G->tickets[kTicketSolve] = 0;
     }
 }
 
@@ -628,9 +662,14 @@ __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
             B.partials[B.n_chunks + c] = mx;
         }
     }
-    if (last_block_done(&B.G->tickets[kTicketSolve], gridDim.x)) {
-        solve_finish(B, which, handle, use_handle, smem);
-        if (threadIdx.x == 0) B.G->tickets[kTicketSolve] = 0;
+    // One scene: its last block finishes the iteration.  Several scenes:
+    // k_solve_finish does, one block per scene.
+    if (B.n_scenes == 1 && last_block_done(&B.G->tickets[kTicketSolve], gridDim.x)) {
+        solve_finish_scene(B, which, 0, 0, smem);
+        if (threadIdx.x == 0) {
+            solve_set_condition(B, which, handle, use_handle);
+            B.G->tickets[kTicketSolve] = 0;
+        }
     }
 }
 
@@ -768,6 +807,56 @@ __device__ __forceinline__ uint32_t fixed_point(float x, float scale) {
     return (uint32_t)v;
 }
 
+// The stats of scene sc from its chunk partials (whole block): two FP64
+// sums in the fixed order, integer max and sums.  c0 = its first chunk.
+__device__ void stats_finish_scene(Bufs& B, const uint4* upart, uint32_t sc, uint32_t c0,
+                                   double* smem, uint32_t (*s_u)[8]) {
+    const DevParams& Q = B.P[sc];
+    uint32_t nch = (Q.n + kBlock - 1) / kBlock;
+    // Two FP64 sums in the fixed order over this scene's chunks.
+    double t1 = 0.0, t2 = 0.0;
+    for (uint32_t k = threadIdx.x; k < nch; k += kBlock) {
+        t1 = t1 + __ldcg(B.partials + 2 * (c0 + k));
+        t2 = t2 + __ldcg(B.partials + 2 * (c0 + k) + 1);
+    }
+    double f1 = block_tree256(t1, smem);
+    double f2 = block_tree256(t2, smem);
+    // integer partials: max and wrapping sums, order-free
+    uint32_t a = 0, b = 0, d = 0;
+    for (uint32_t k = threadIdx.x; k < nch; k += kBlock) {
+        uint4 u = __ldcg(upart + c0 + k);
+        a = max(a, u.x);
+        b += u.y;
+        d += u.z;
+    }
+    for (int m = 16; m >= 1; m >>= 1) {
+        a = max(a, __shfl_xor_sync(kFull, a, m));
+        b += __shfl_xor_sync(kFull, b, m);
+        d += __shfl_xor_sync(kFull, d, m);
+    }
+    if (lane_id() == 0) {
+        s_u[0][threadIdx.x >> 5] = a;
+        s_u[1][threadIdx.x >> 5] = b;
+        s_u[2][threadIdx.x >> 5] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a = b = d = 0;
+        for (int w = 0; w < 8; ++w) {
+            a = max(a, s_u[0][w]);
+            b += s_u[1][w];
+            d += s_u[2][w];
+        }
+        SceneState& S = B.S[sc];
+        S.stats[0] = a;
+        S.stats[1] = b;
+        S.stats[2] = d;
+        S.stats_f64[0] = f1 / (double)Q.n;
+        S.stats_f64[1] = f2 / (double)Q.n;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upart) {
     __shared__ double smem[8];
     __shared__ uint32_t s_u[3][8];
@@ -816,56 +905,20 @@ __global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upar
         B.partials[2 * c] = p1;
         B.partials[2 * c + 1] = p2;
     }
-    if (last_block_done(&B.G->tickets[kTicketStats], gridDim.x)) {
-        uint32_t c0 = 0;
-        for (uint32_t sc = 0; sc < B.n_scenes; ++sc) {
-            const DevParams& Q = B.P[sc];
-            uint32_t nch = (Q.n + kBlock - 1) / kBlock;
-            // Two FP64 sums in the fixed order over this scene's chunks.
-            double t1 = 0.0, t2 = 0.0;
-            for (uint32_t k = threadIdx.x; k < nch; k += kBlock) {
-                t1 = t1 + __ldcg(B.partials + 2 * (c0 + k));
-                t2 = t2 + __ldcg(B.partials + 2 * (c0 + k) + 1);
-            }
-            double f1 = block_tree256(t1, smem);
-            double f2 = block_tree256(t2, smem);
-            // integer partials: max and wrapping sums, order-free
-            uint32_t a = 0, b = 0, d = 0;
-            for (uint32_t k = threadIdx.x; k < nch; k += kBlock) {
-                uint4 u = __ldcg(upart + c0 + k);
-                a = max(a, u.x);
-                b += u.y;
-                d += u.z;
-            }
-            for (int m = 16; m >= 1; m >>= 1) {
-                a = max(a, __shfl_xor_sync(kFull, a, m));
-                b += __shfl_xor_sync(kFull, b, m);
-                d += __shfl_xor_sync(kFull, d, m);
-            }
-            if (lane_id() == 0) {
-                s_u[0][threadIdx.x >> 5] = a;
-                s_u[1][threadIdx.x >> 5] = b;
-                s_u[2][threadIdx.x >> 5] = d;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                a = b = d = 0;
-                for (int w = 0; w < 8; ++w) {
-                    a = max(a, s_u[0][w]);
-                    b += s_u[1][w];
-                    d += s_u[2][w];
-                }
-                SceneState& S = B.S[sc];
-                S.stats[0] = a;
-                S.stats[1] = b;
-                S.stats[2] = d;
-                S.stats_f64[0] = f1 / (double)Q.n;
-                S.stats_f64[1] = f2 / (double)Q.n;
-            }
-            c0 += nch;
-        }
+    // One scene: its last block finishes.  Several scenes: k_stats_finish
+    // does, one block per scene.
+    if (B.n_scenes == 1 && last_block_done(&B.G->tickets[kTicketStats], gridDim.x)) {
+        stats_finish_scene(B, upart, 0, 0, smem, s_u);
         if (threadIdx.x == 0) B.G->tickets[kTicketStats] = 0;
     }
+}
+
+__global__ void __launch_bounds__(kBlock) k_stats_finish(Bufs B, uint4* upart) {
+    __shared__ double smem[8];
+    __shared__ uint32_t s_u[3][8];
+    const uint32_t sc = blockIdx.x;
+    const uint32_t c0 = scene_chunk_base(B, sc, s_u[0]);
+    stats_finish_scene(B, upart, sc, c0, smem, s_u);
 }
 
 // ---------------------------------------------------------------------------

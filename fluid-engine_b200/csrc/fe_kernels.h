@@ -20,6 +20,10 @@ __global__ void k_take_pressure_carry(Bufs B, LearnArgs L);
 __global__ void k_refresh_pr(Bufs B);
 __global__ void k_density_alpha(Bufs B);
 __global__ void k_viscosity(Bufs B);
+// Per-scene finishes of a multi-scene context, one block per scene.
+__global__ void k_solve_finish(Bufs B, int which, cudaGraphConditionalHandle handle,
+                               int use_handle);
+__global__ void k_stats_finish(Bufs B, uint4* upart);
 __global__ void k_density_source(Bufs B);
 __global__ void k_divergence_source(Bufs B, int fixed);
 __global__ void k_pressure_force(Bufs B, int which);
