@@ -166,6 +166,40 @@ class ClockSampler:
                 "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
+def free_port() -> int:
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def spawn_command(gpus: int, env, argv, device_count: int, needs_gpus: bool = True):
+    """The command that starts `gpus` ranks of this script (one per GPU,
+    torch.distributed.run on 127.0.0.1) when no launcher started this process
+    (WORLD_SIZE unset), or None when this process already is a rank or one
+    GPU is asked for.  SystemExit (non-zero) when the request cannot be met:
+    a launcher's WORLD_SIZE that disagrees with --gpus, or fewer GPUs than
+    ranks."""
+    world = env.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != gpus:
+            raise SystemExit(f"bench.py: --gpus {gpus} but the launcher started "
+                             f"WORLD_SIZE={world} ranks")
+        return None
+    if gpus < 1:
+        raise SystemExit(f"bench.py: --gpus {gpus} is not a rank count")
+    if gpus == 1:
+        return None
+    if needs_gpus and device_count < gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but only {device_count} CUDA device(s) "
+                         f"are visible")
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={gpus}", "--master-addr", "127.0.0.1",
+            "--master-port", str(free_port()), os.path.abspath(__file__)] + list(argv)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -453,44 +487,57 @@ def run_batch(args, world, rank, local):
     over ranks and the value counts every scene's particles (strong scaling:
     the 64 scenes are fixed).  At N=1 the same scenes also run as 64 separate
     contexts stepped one after another, for comparison.  Per-scene stats are
-    all-gathered after the timed region."""
+    all-gathered after the timed region (fluid_step.sharding.run_scene_shard)."""
     import torch
 
     from fluid_step import scene
     from fluid_step.pipelines import BatchSimulation, Simulation
-    from fluid_step.sharding import gather_scene_stats, imbalance, lpt_partition, stats_row
+    from fluid_step.sharding import run_scene_shard
 
     w = scene.batch_workload()
-    parts = lpt_partition(w.counts, world)
-    mine = parts[rank]
     pos, par = w.positions(), w.params()
     total = int(sum(w.counts))
-    sim = BatchSimulation([pos[k] for k in mine], [par[k] for k in mine], device=local)
-    lib, h = sim.data._lib, sim.data.handle
-    stream = torch.cuda.ExternalStream(lib.fe_get_stream(h), device=local)
-    for _ in range(args.warmup):
-        sim.step(1)
-    barrier(world)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        a.record(stream)
-        for _ in range(args.steps):
-            rc = lib.fe_step(h, 1, 0, None)
-            if rc:
-                raise RuntimeError(f"fe_step (batch) failed: {rc}")
-        b.record(stream)
-        b.synchronize()
-    ms = reduce_max(a.elapsed_time(b), world)
-    rows = [stats_row(sim.data.read_scene_stats(i)) for i in range(len(mine))]
-    sim.close()
-    table = gather_scene_stats(mine, rows, len(w.counts),
-                               device=f"cuda:{local}" if world > 1 else None)
+    clocks = ClockSampler(local)
+
+    class GpuShard:
+        def __init__(self, mine):
+            self.sim = BatchSimulation([pos[k] for k in mine], [par[k] for k in mine],
+                                       device=local)
+            self.lib, self.h = self.sim.data._lib, self.sim.data.handle
+            self.stream = torch.cuda.ExternalStream(self.lib.fe_get_stream(self.h),
+                                                    device=local)
+
+        def step(self):
+            self.sim.step(1)
+
+        def timed_steps(self, k):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with clocks:
+                a.record(self.stream)
+                for _ in range(k):
+                    rc = self.lib.fe_step(self.h, 1, 0, None)
+                    if rc:
+                        raise RuntimeError(f"fe_step (batch) failed: {rc}")
+                b.record(self.stream)
+                b.synchronize()
+            return a.elapsed_time(b) / 1e3
+
+        def scene_stats(self, i):
+            return self.sim.data.read_scene_stats(i)
+
+        def close(self):
+            self.sim.close()
+
+    res = run_scene_shard(w.counts, rank, world, GpuShard, args.steps, args.warmup,
+                          device=f"cuda:{local}" if world > 1 else None)
+    ms = res["seconds"] * 1e3
+    table = res["table"]
     out = {"workload": w.name, "scenes": len(w.counts), "particles": total,
            "counts_min_max": [min(w.counts), max(w.counts)],
            "value": total * args.steps / (ms / 1e3), "unit": "particle-steps/s",
            "ms_per_step": ms / args.steps, "scaling": "strong", "ranks": world,
-           "partition_imbalance": imbalance(w.counts, parts),
+           "partition_imbalance": res["imbalance"],
            "physics": "dt 1 ms, 4 + 4 Jacobi iterations, REFERENCE mode, radix sort, "
                       "per-scene XSPH coefficient",
            "non_finite_scenes": int(np.sum(table[:, -1].astype(np.int64) & 0x8 != 0)),
@@ -611,7 +658,8 @@ def run_gpu(args) -> None:
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(args.workload, w)
+            cpu = cpu_baseline(args.workload, w,
+                               untimed=args.warmup + (1 if args.autotune else 0))
         variant = "learned warm start" if "learned" in arms else "plain Jacobi"
         out = {
             "metric": "DFSPH particle-steps/s (Jacobi to 0.1% density and divergence error)",
@@ -675,9 +723,11 @@ def run_gpu(args) -> None:
         dist.destroy_process_group()
 
 
-def cpu_baseline(workload: str, w=None, frames: int = 1):
-    """The oracle (FP32 shader-order C++ port, OpenMP) on the same workload:
-    `frames` frames from rest, timed with the host clock."""
+def cpu_baseline(workload: str, w=None, untimed: int = 0, frames: int = 3):
+    """The oracle (FP32 shader-order C++ port, OpenMP over every core the
+    process may use) on the same workload: `untimed` frames from rest, then
+    `frames` frames timed with the host clock (a bounded sample of the GPU
+    arm's timed window)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -685,13 +735,16 @@ def cpu_baseline(workload: str, w=None, frames: int = 1):
     w = w or scene.workload(workload)
     pos = w.positions()
     o = oracle.Oracle(w.params, pos)
+    for _ in range(untimed):
+        o.step(1)
     t0 = time.perf_counter()
     for _ in range(frames):
         o.step(1)
     dt = time.perf_counter() - t0
     return {"value": pos.shape[0] * frames / dt, "unit": "particle-steps/s",
             "cores": oracle.get_threads(), "kind": "port",
-            "sample": f"{frames} frame(s) of {workload} ({pos.shape[0]} particles) from rest"}
+            "sample": f"frames {untimed + 1}..{untimed + frames} of {workload} "
+                      f"({pos.shape[0]} particles) after {untimed} untimed frames from rest"}
 
 
 def run_profile_passes(args) -> None:
@@ -795,6 +848,11 @@ def run_profile_render(args) -> None:
 
 
 def run_reference(args) -> None:
+    """The reference algorithm on the host cores (the oracle, OpenMP over
+    every core the process may use), on the GPU arm's frames: the GPU arm
+    runs one frame to tune on (unless --no-autotune) and W warm-up frames
+    before its K timed frames, so this arm runs 1 + W untimed frames and
+    then times the same K frames.  Under a launcher only rank 0 works."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
@@ -804,10 +862,11 @@ def run_reference(args) -> None:
     w = scene.workload(args.workload)
     pos = w.positions()
     o = oracle.Oracle(w.params, pos)
-    for _ in range(min(args.warmup, 1)):
+    untimed = args.warmup + (1 if args.autotune else 0)
+    for _ in range(untimed):
         o.step(1)
+    steps = max(1, args.steps)
     t0 = time.perf_counter()
-    steps = max(1, min(args.steps, args.reference_steps))
     for _ in range(steps):
         o.step(1)
     dt = time.perf_counter() - t0
@@ -815,14 +874,19 @@ def run_reference(args) -> None:
     out = {"impl": "reference",
            "metric": "DFSPH particle-steps/s (Jacobi to 0.1% density and divergence error)",
            "value": v, "unit": "particle-steps/s", "n_gpus": world, "steps": steps,
-           "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3 / steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3 / steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic: seeded dam-break lattice, random jitter +-0.005",
-           "config": {"workload": args.workload, "particles_per_gpu": pos.shape[0]},
+           "data": "synthetic: seeded dam-break lattice, jitter +-0.005, at rest",
+           "config": {"workload": args.workload, "particles_per_gpu": pos.shape[0],
+                      "variant": "plain Jacobi (the reference has no learned warm start)",
+                      "mode": "FIXED" if w.params.mode == 1 else "REFERENCE",
+                      "frames": f"{untimed + 1}..{untimed + steps} of the run from rest, "
+                                f"the GPU arm's timed window"},
            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": oracle.get_threads(),
                             "kind": "port",
-                            "sample": f"{steps} frame(s) of {args.workload} after "
-                                      f"{min(args.warmup, 1)} warm-up frame"},
+                            "sample": f"frames {untimed + 1}..{untimed + steps} of "
+                                      f"{args.workload} ({pos.shape[0]} particles), after "
+                                      f"{untimed} untimed frames from rest"},
            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -835,7 +899,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="dam_break_1m")
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
-    ap.add_argument("--reference-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", default="both", choices=["both", "learned", "plain"],
                     help="learned warm start, plain Jacobi, or both (value = learned)")
@@ -859,6 +922,15 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    device_count = 0
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        import torch
+        device_count = torch.cuda.device_count()
+    cmd = spawn_command(args.gpus, os.environ, sys.argv[1:], device_count,
+                        needs_gpus=args.impl != "reference")
+    if cmd:
+        # one process per GPU; rank 0 prints the JSON line
+        sys.exit(subprocess.run(cmd).returncode)
     if args.profile_passes:
         run_profile_passes(args)
     elif args.profile_sort:

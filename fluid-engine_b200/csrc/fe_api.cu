@@ -1615,6 +1615,8 @@ fe_status sort_pairs_impl(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t k
     } else {
         FE_CUDA(cudaStreamWaitEvent(stream, S.done, 0));
     }
+    // the error word reports this call only (fe_sort_flags reads it)
+    REC(R.fill_u32(S.flags, 0u, 8));
     bool in_tmp = false;
     REC(radix_sort(L, keys, vals, S.tk, S.tv, n, kb, S.words, S.flags, &in_tmp, cfg));
     if (in_tmp) {
@@ -1631,6 +1633,31 @@ fe_status fe_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t key
                         int algorithm, void* stream_ptr) {
     NvtxRange range_("fe_sort_pairs");
     return sort_pairs_impl(keys, vals, n, key_bits, algorithm, stream_ptr, nullptr);
+}
+
+// Error word of the last radix fe_sort_pairs on the current device, copied
+// in the order of `stream` after that sort (0 before any radix sort).
+fe_status fe_sort_flags(uint32_t* flags_out, void* stream_ptr) {
+    if (!flags_out) {
+        set_error("fe_sort_flags: NULL flags_out");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    int dev;
+    FE_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 16) {
+        set_error("device index %d unsupported", dev);
+        return FE_ERR_NO_DEVICE;
+    }
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    std::lock_guard<std::mutex> lock(g_sort_mutex);
+    SortScratch& S = g_sort[dev];
+    if (!S.flags) {
+        FE_CUDA(cudaMemsetAsync(flags_out, 0, sizeof(uint32_t), stream));
+        return FE_OK;
+    }
+    FE_CUDA(cudaStreamWaitEvent(stream, S.done, 0));
+    FE_CUDA(cudaMemcpyAsync(flags_out, S.flags, sizeof(uint32_t), cudaMemcpyDefault, stream));
+    return FE_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1812,12 +1839,18 @@ fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_
         s = FE_ERR_CUDA;
     }
     if (s == FE_OK) s = fe_sort_pairs(dk, dv, n, key_bits, algorithm, st);
+    uint32_t flags = 0;
+    if (s == FE_OK && algorithm == FE_SORT_RADIX) s = fe_sort_flags(&flags, st);
     if (s == FE_OK &&
         (cudaMemcpyAsync(keys, dk, (size_t)n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
          cudaMemcpyAsync(vals, dv, (size_t)n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
          cudaStreamSynchronize(st) != cudaSuccess)) {
         set_error("device-to-host copy failed");
         s = FE_ERR_CUDA;
+    }
+    if (s == FE_OK && (flags & FE_STATS_LOOKBACK_TIMEOUT)) {
+        set_error("fe_sort_pairs_host: a bounded look-back wait gave up; the output is not valid");
+        s = FE_ERR_TIMEOUT;
     }
     if (st) {
         cudaStreamSynchronize(st);

@@ -476,6 +476,13 @@ cudaError_t lookback_wait_selftest(int limit, uint32_t* flags_out) {
     return e;
 }
 
+cudaError_t lookback_wait_on(uint32_t* status, uint32_t* error_flags, int limit,
+                             cudaStream_t stream) {
+    k_lookback_selftest<<<1, 1, 0, stream>>>(status, error_flags,
+                                             limit < kMaxSpins ? limit : kMaxSpins);
+    return cudaGetLastError();
+}
+
 cudaError_t bitonic_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, uint32_t n) {
     if (n < 2) return cudaSuccess;
     if (n & (n - 1)) return cudaErrorInvalidValue;

@@ -68,4 +68,9 @@ cudaError_t bitonic_sort(const SortLaunch& L, uint32_t* keys, uint32_t* vals, ui
 // device; *flags_out receives the error flags it raised (0x4 = timed out).
 cudaError_t lookback_wait_selftest(int limit, uint32_t* flags_out);
 
+// The same wait, enqueued on `stream`, on a caller's status word (which must
+// hold no published flag) with the timeout flag raised in *error_flags.
+cudaError_t lookback_wait_on(uint32_t* status, uint32_t* error_flags, int limit,
+                             cudaStream_t stream);
+
 }  // namespace fe

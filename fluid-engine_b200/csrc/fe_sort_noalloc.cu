@@ -10,6 +10,7 @@
 // back.  fe_sort_pairs_noalloc sorts with a scratch area that is a file-scope
 // __device__ array: the CUDA runtime reserves it on each GPU when the library
 // is loaded there, and it stays reserved until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -35,25 +36,75 @@ constexpr size_t kWords = 2u * (size_t)kMaxPairs + kRadixWords + 8u;
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
 
 std::mutex g_mutex;
-uint32_t* g_scratch_ptr[kMaxDevices] = {};
+
+// Per device: the CUDA context the address below was looked up in, and that
+// address.  A device reset (cudaDeviceReset, or the primary context being
+// destroyed and made again) loads the library's module anew, and the array
+// may then live at another address; the context's unique ID tells a new
+// context from the old one even if its handle value were reused.
+struct ScratchAddress {
+    unsigned long long ctx_id = 0;
+    bool valid = false;
+    uint32_t* ptr = nullptr;
+};
+ScratchAddress g_scratch[kMaxDevices];
+
+// The driver's cuCtxGetCurrent and cuCtxGetId, fetched through the runtime
+// (the library does not link the driver library directly).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+cudaError_t current_context_id(unsigned long long* id) {
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+        if (e != cudaSuccess) return e;
+        if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+            return cudaErrorSymbolNotFound;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return cudaErrorDeviceUninitialized;
+    if (g_ctx_get_id(ctx, id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
 
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the symbol's name is only a host-side handle, never a device address, so
-// the address is looked up once per device, with that device current.
+// the address is looked up with the device current: on the first call in
+// each CUDA context of a device (normally once per device per process).
 cudaError_t scratch_for_current_device(uint32_t** out, int* device) {
     cudaError_t e = cudaGetDevice(device);
     if (e != cudaSuccess) return e;
     if (*device < 0 || (uint32_t)*device >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[*device]) {
-        uint32_t* p = nullptr;
-        e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[*device] = p;
+    ScratchAddress& a = g_scratch[*device];
+    unsigned long long id = 0;
+    if (a.valid && current_context_id(&id) == cudaSuccess && id == a.ctx_id) {
+        *out = a.ptr;
+        return cudaSuccess;
     }
-    *out = g_scratch_ptr[*device];
+    // First call in this context (the lookup also makes the device's primary
+    // context current in a thread that has not used the runtime yet).
+    uint32_t* p = nullptr;
+    if ((e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch)) != cudaSuccess) return e;
+    if ((e = current_context_id(&id)) != cudaSuccess) return e;
+    a.ptr = p;
+    a.ctx_id = id;
+    a.valid = true;
+    *out = p;
     return cudaSuccess;
 }
+
+// The error word of the last call inside the scratch (see the layout above).
+uint32_t* flags_word(uint32_t* scratch) { return scratch + 2u * (size_t)kMaxPairs + kRadixWords; }
 
 struct EagerLaunch {
     cudaStream_t stream;
@@ -103,7 +154,7 @@ extern "C" FE_API fe_status fe_sort_pairs_noalloc(uint32_t* keys, uint32_t* valu
     uint32_t* tmp_keys = scratch;
     uint32_t* tmp_vals = scratch + kMaxPairs;
     uint32_t* radix_words = scratch + 2u * (size_t)kMaxPairs;
-    uint32_t* flags = radix_words + kRadixWords;
+    uint32_t* flags = flags_word(scratch);
     EagerLaunch ctx{(cudaStream_t)stream_ptr};
     fe::SortLaunch L{&ctx, launch_on_stream, fill_on_stream};
     e = L.fill(flags, 0u, 8);
@@ -119,6 +170,52 @@ extern "C" FE_API fe_status fe_sort_pairs_noalloc(uint32_t* keys, uint32_t* valu
     }
     if (e != cudaSuccess) {
         fe_set_error_message("fe_sort_pairs_noalloc: %s", cudaGetErrorString(e));
+        return FE_ERR_CUDA;
+    }
+    return FE_OK;
+}
+
+// The error word of the last fe_sort_pairs_noalloc call on the current
+// device, copied in the order of `stream`.
+extern "C" FE_API fe_status fe_sort_noalloc_flags(uint32_t* flags_out, void* stream_ptr) {
+    if (!flags_out) {
+        fe_set_error_message("fe_sort_noalloc_flags: NULL flags_out");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    uint32_t* scratch = nullptr;
+    int device = -1;
+    cudaError_t e = scratch_for_current_device(&scratch, &device);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(flags_out, flags_word(scratch), sizeof(uint32_t), cudaMemcpyDefault,
+                            (cudaStream_t)stream_ptr);
+    if (e != cudaSuccess) {
+        fe_set_error_message("fe_sort_noalloc_flags on device %d: %s", device,
+                             cudaGetErrorString(e));
+        return FE_ERR_CUDA;
+    }
+    return FE_OK;
+}
+
+// Test hook: the radix pass's bounded look-back wait, run on a status word
+// of the static scratch that nobody publishes, raising its timeout flag in
+// the same error word a sort would.  No GPU fault is involved: the wait gives
+// up after `limit` polls.
+extern "C" FE_API fe_status fe_debug_noalloc_wait_timeout(uint32_t limit, void* stream_ptr) {
+    if (limit == 0) {
+        fe_set_error_message("fe_debug_noalloc_wait_timeout needs a non-zero limit");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    uint32_t* scratch = nullptr;
+    int device = -1;
+    cudaError_t e = scratch_for_current_device(&scratch, &device);
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    uint32_t* flags = flags_word(scratch);
+    if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, 8 * sizeof(uint32_t), stream);
+    if (e == cudaSuccess)
+        e = fe::lookback_wait_on(flags + 1, flags, (int)(limit < (1u << 30) ? limit : (1u << 30)),
+                                 stream);
+    if (e != cudaSuccess) {
+        fe_set_error_message("fe_debug_noalloc_wait_timeout: %s", cudaGetErrorString(e));
         return FE_ERR_CUDA;
     }
     return FE_OK;

@@ -327,6 +327,9 @@ SIGNATURES = {
     "fe_sort_pairs": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p]),
     "fe_sort_pairs_host": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_int]),
     "fe_sort_pairs_noalloc": (c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p]),
+    "fe_sort_noalloc_flags": (c_int, [c_void_p, c_void_p]),
+    "fe_sort_flags": (c_int, [c_void_p, c_void_p]),
+    "fe_debug_noalloc_wait_timeout": (c_int, [c_uint32, c_void_p]),
     "fe_model_create": (c_int, [c_uint32, c_int, POINTER(c_void_p)]),
     "fe_model_destroy": (c_int, [c_void_p]),
     "fe_model_set_parameters": (c_int, [c_void_p, c_void_p, c_size_t]),

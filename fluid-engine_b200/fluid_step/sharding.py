@@ -76,3 +76,55 @@ def gather_scene_stats(local_scenes, local_rows, n_scenes: int, group=None, devi
     if np.isnan(buf[:, -1]).any():
         raise RuntimeError("a scene has no owner rank")
     return buf[:, :-1]
+
+
+def _dist_ready() -> bool:
+    import torch.distributed as dist
+    return dist.is_available() and dist.is_initialized()
+
+
+def max_over_ranks(value: float, device=None, group=None) -> float:
+    """The largest `value` over the ranks of the process group (the value
+    itself without one)."""
+    if not _dist_ready():
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64)
+    if device is not None:
+        t = t.to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
+def run_scene_shard(work, rank: int, world: int, open_shard, steps: int, warmup: int,
+                    device=None, group=None) -> dict:
+    """One rank's part of a scene-sharded run.
+
+    The rank takes its LPT share of the scenes (`work` = particles per scene),
+    opens one batch over them with open_shard(scene_indices), runs `warmup`
+    untimed steps, then `steps` timed ones (shard.timed_steps(k) returns the
+    seconds its own clock measured), and closes it.  The time is the maximum
+    over ranks; the per-scene stats rows are all-gathered into the table of
+    every scene.  Every rank makes the same collective calls in the same
+    order: a barrier before the timed steps, the max, the gather.
+
+    The shard object provides step(), timed_steps(k) -> seconds,
+    scene_stats(i) -> FeStats of its i-th scene, close()."""
+    parts = lpt_partition(work, world)
+    mine = parts[rank]
+    shard = open_shard(mine)
+    try:
+        for _ in range(warmup):
+            shard.step()
+        if _dist_ready():
+            import torch.distributed as dist
+            dist.barrier(group=group)
+        seconds = shard.timed_steps(steps)
+        rows = [stats_row(shard.scene_stats(i)) for i in range(len(mine))]
+    finally:
+        shard.close()
+    seconds = max_over_ranks(seconds, device=device, group=group)
+    table = gather_scene_stats(mine, rows, len(work), group=group, device=device)
+    return {"parts": parts, "mine": mine, "seconds": seconds, "table": table,
+            "imbalance": imbalance(work, parts)}

@@ -440,6 +440,14 @@ FE_API fe_status fe_step(fe_ctx* ctx, uint32_t n_substeps, uint32_t flags, fe_st
  * Scratch is allocated on first use per (device, size class) and kept. */
 FE_API fe_status fe_sort_pairs(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
                         uint32_t key_bits, int algorithm, void* stream);
+/* Error word (FE_STATS_* bits) of the last radix fe_sort_pairs on the
+ * current device, copied to *flags_out (host or device memory) in the order
+ * of `stream`, after that sort: the value is there once `stream` has reached
+ * this point (for host memory, synchronise the stream first).
+ * FE_STATS_LOOKBACK_TIMEOUT means a bounded look-back wait of that sort gave
+ * up and its output is not valid.  Each radix call clears the word first.
+ * No counterpart in the reference (its sort has no failure path). */
+FE_API fe_status fe_sort_flags(uint32_t* flags_out, void* stream);
 
 /* ------------------------------------------------------------------------- */
 /* Autotuning (no reference counterpart: the reference fixes its workgroup   */
@@ -493,7 +501,8 @@ FE_API fe_status fe_sort_pairs_config(uint32_t* d_keys, uint32_t* d_values, uint
                                       void* stream);
 
 /* Same as fe_sort_pairs with host arrays: copies in, sorts, copies out
- * (in place). */
+ * (in place).  FE_ERR_TIMEOUT when the radix sort's bounded look-back wait
+ * gave up (the arrays then hold no valid result). */
 FE_API fe_status fe_sort_pairs_host(uint32_t* keys, uint32_t* values, uint32_t n,
                              uint32_t key_bits, int algorithm);
 
@@ -561,14 +570,30 @@ FE_API fe_status fe_capture_end(fe_ctx* ctx);
  * Same result as fe_sort_pairs with FE_SORT_RADIX.  Its scratch is a static
  * device array of about 9 MiB that every GPU loading the library holds until
  * the process exits; n above FE_SORT_NOALLOC_MAX_PAIRS returns
- * FE_ERR_CAPACITY.  The first call on a device looks up the array's device
- * address (make that first call before any stream capture).  All calls share
+ * FE_ERR_CAPACITY.  The first call in a device's CUDA context looks up the
+ * array's device address (make that first call before any stream capture;
+ * after a device reset the next call looks it up again).  All calls share
  * the array, so calls that overlap on the GPU (concurrent streams, devices
- * excepted) race; serialise them on one stream.  keys and values are device
+ * excepted) race.  Unlike fe_sort_pairs, which orders its callers through an
+ * event, this entry point does no ordering across streams: serialise calls
+ * on one stream, or order calls on different streams yourself (for example
+ * with cudaEventRecord / cudaStreamWaitEvent).  keys and values are device
  * pointers of the current device; work is enqueued on `stream`. */
 #define FE_SORT_NOALLOC_MAX_PAIRS (1u << 20)
 FE_API fe_status fe_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_values, uint32_t n,
                                        uint32_t key_bits, void* stream);
+/* Error word (FE_STATS_* bits) of the last fe_sort_pairs_noalloc call on the
+ * current device, copied from the static array to *flags_out (host or device
+ * memory) in the order of `stream`; for host memory, synchronise the stream
+ * before reading it.  FE_STATS_LOOKBACK_TIMEOUT means that call's bounded
+ * look-back wait gave up and its output is not valid.  Each call clears the
+ * word first; allocates nothing.  No counterpart in the reference. */
+FE_API fe_status fe_sort_noalloc_flags(uint32_t* flags_out, void* stream);
+/* Test hook: runs the radix pass's bounded look-back wait, on `stream`, on a
+ * word of the static array that nothing publishes, so that it gives up after
+ * `limit` polls and raises FE_STATS_LOOKBACK_TIMEOUT in the error word that
+ * fe_sort_noalloc_flags reports.  No GPU fault is involved. */
+FE_API fe_status fe_debug_noalloc_wait_timeout(uint32_t limit, void* stream);
 
 #ifdef __cplusplus
 }

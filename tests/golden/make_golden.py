@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures from the reference's own CSV outputs.
 
-Run in a container where the reference is mounted:
-    python tests/golden/make_golden.py /root/reference
+Run where the reference project is checked out, giving its root (or set
+FE_REFERENCE_ROOT):
+    python tests/golden/make_golden.py <reference project root>
 Writes:
   rest_density.npy     float32[4800]: scripts/rest_density.csv, the densities
                        after one neighbour search (bitonic) + density_alpha
@@ -49,4 +50,8 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FE_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference project root> "
+                 "(or set FE_REFERENCE_ROOT)")
+    main(root)

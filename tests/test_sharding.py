@@ -90,3 +90,86 @@ def test_gather_without_process_group_returns_local_rows():
     t = gather_scene_stats([0, 2], rows, 3)
     assert np.array_equal(t[0], rows[0]) and np.array_equal(t[2], rows[1])
     assert np.all(t[1] == 0)
+
+
+class _StandInShard:
+    """A CPU stand-in for one rank's batch context: each step advances every
+    scene of the share; a scene's stats name the scene and its step count,
+    so the gathered table shows which rank ran which scene how often."""
+
+    def __init__(self, mine, counts):
+        self.mine, self.counts, self.steps = list(mine), counts, 0
+
+    def step(self):
+        self.steps += 1
+
+    def timed_steps(self, k):
+        import time
+        t0 = time.perf_counter()
+        for _ in range(k):
+            self.step()
+        # make the ranks' times differ, so that the max over ranks shows
+        return time.perf_counter() - t0 + 1e-6 * sum(self.counts[s] for s in self.mine)
+
+    def scene_stats(self, i):
+        from fluid_step import _abi
+        st = _abi.FeStats()
+        k = self.mine[i]
+        st.max_speed = float(k)
+        st.dt = 1e-3 * (k + 1)
+        st.substeps = self.steps
+        st.density_iterations = self.counts[k] % 97
+        return st
+
+    def close(self):
+        pass
+
+
+def _shard_rank_main(rank, world, port, counts, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    from fluid_step.sharding import run_scene_shard
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        res = run_scene_shard(counts, rank, world, lambda mine: _StandInShard(mine, counts),
+                              steps=5, warmup=3)
+        own = 1e-6 * sum(counts[s] for s in res["mine"])
+        q.put((rank, res["mine"], res["seconds"], own, res["table"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_batch_run_two_gloo_ranks():
+    """The scene-sharded run path end to end on two gloo ranks: the LPT
+    partition, a per-rank stand-in for the batch step (warm-up, timed steps),
+    the time as the max over ranks and the gathered per-scene table."""
+    import torch.multiprocessing as mp
+
+    from fluid_step.sharding import STAT_FIELDS
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    counts = scene.batch_workload(n_scenes=11).counts
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_rank_main, args=(r, 2, port, counts, q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    parts = lpt_partition(counts, 2)
+    assert [r[1] for r in results] == parts
+    # the time every rank reports is the larger of the two ranks' own
+    assert results[0][2] == results[1][2] >= max(r[3] for r in results)
+    col = {f: i for i, f in enumerate(STAT_FIELDS)}
+    for rank, mine, _, _, table in results:
+        assert table.shape == (len(counts), len(STAT_FIELDS))
+        assert np.array_equal(table[:, col["max_speed"]], np.arange(len(counts)))
+        assert np.all(table[:, col["substeps"]] == 3 + 5)   # warm-up + timed, every scene
+        assert np.array_equal(table[:, col["density_iterations"]], np.array(counts) % 97)
