@@ -129,6 +129,17 @@ struct Recorder {
         ((p[I] = (void*)&std::get<I>(t)), ...);
     }
 
+    // Device-to-device copy in recording order.
+    cudaError_t copy(void* dst, const void* src, size_t bytes) {
+        if (!graph) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream);
+        cudaGraphNode_t node;
+        cudaError_t e = cudaGraphAddMemcpyNode1D(&node, graph, last ? &last : nullptr,
+                                                 last ? 1 : 0, dst, src, bytes,
+                                                 cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) last = node;
+        return e;
+    }
+
     cudaError_t fill_u32(uint32_t* p, uint32_t v, size_t count) {
         if (count == 0) return cudaSuccess;
         size_t blocks = std::min<size_t>((count + 255) / 256, 148 * 8);
@@ -288,6 +299,10 @@ struct fe_ctx {
     fe_model* model = nullptr;       // attached, not owned
     LearnArgs L{};
     bool capture = false;
+    // test hook fe_debug_trace_learned: per solve slot, the network's input
+    // rows (n x 32 B) and outputs (n x 8 B) as the warm start used them
+    unsigned char* trace = nullptr;
+    uint32_t trace_slots = 0, trace_cap = 0;
 
     // density splat: headless grid and the non-zero taps of the splat kernel
     uint32_t* splat_grid = nullptr;
@@ -501,8 +516,20 @@ fe_status rec_mlp(fe_ctx* c, Recorder& R) {
     return FE_OK;
 }
 
-// One substep of Renderer::step (renderer/mod.rs:289-337).
-fe_status rec_substep(fe_ctx* c, Recorder& R) {
+// Test hook: records the network's input rows and outputs of solve slot
+// `slot` (2 x substep + which) into the trace buffer.
+constexpr size_t kTraceBytesPerParticle = 16 * 2 + 2 * 4;
+fe_status rec_trace(fe_ctx* c, Recorder& R, uint32_t slot) {
+    if (slot >= c->trace_slots) return FE_OK;
+    unsigned char* base = c->trace + (size_t)slot * c->n * kTraceBytesPerParticle;
+    REC(R.copy(base, c->L.xb, (size_t)c->n * 32));
+    REC(R.copy(base + (size_t)c->n * 32, c->L.out, (size_t)c->n * 8));
+    return FE_OK;
+}
+
+// One substep of Renderer::step (renderer/mod.rs:289-337); k = its index in
+// the frame.
+fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     Bufs B = c->B;
     const int fixed = c->fixed_mode() ? 1 : 0;
     fe_status s;
@@ -513,6 +540,7 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
         return s;
     if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
+        if ((s = rec_trace(c, R, 2 * k))) return s;
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 0));
     }
     if ((s = rec_solve(c, R, 0))) return s;
@@ -530,6 +558,7 @@ fe_status rec_substep(fe_ctx* c, Recorder& R) {
         REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));
     if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
+        if ((s = rec_trace(c, R, 2 * k + 1))) return s;
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 1));
     }
     if ((s = rec_solve(c, R, 1))) return s;
@@ -549,7 +578,7 @@ fe_status rec_frame(fe_ctx* c, Recorder& R, uint32_t n_substeps, bool init) {
         if ((s = rec_simple(c, R, k_density_alpha))) return s;
     }
     for (uint32_t k = 0; k < n_substeps; ++k)
-        if ((s = rec_substep(c, R))) return s;
+        if ((s = rec_substep(c, R, k))) return s;
     return rec_stats(c, R);
 }
 
@@ -634,7 +663,7 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
 uint64_t graph_key(const fe_ctx* c, uint32_t n_substeps, bool init) {
     return (uint64_t)n_substeps | ((uint64_t)init << 32) | ((uint64_t)c->sort_algorithm() << 33) |
            ((uint64_t)c->fixed_mode() << 34) | ((uint64_t)c->learned() << 35) |
-           ((uint64_t)c->capture << 36);
+           ((uint64_t)c->capture << 36) | ((uint64_t)c->trace_slots << 40);
 }
 
 fe_status get_graph(fe_ctx* c, uint32_t n_substeps, bool init, cudaGraphExec_t* out) {
@@ -1522,6 +1551,45 @@ FE_API fe_status fe_capture_end(fe_ctx* c) {
     drop_graphs(c);
     c->capture = false;
     c->L.capture = 0;
+    return FE_OK;
+}
+
+FE_API fe_status fe_debug_trace_learned(fe_ctx* c, uint32_t slots) {
+    if (!c) {
+        set_error("fe_debug_trace_learned: context is NULL");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    if (slots > 64) {
+        set_error("fe_debug_trace_learned: at most 64 solve slots");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    if (slots > c->trace_cap) {
+        unsigned char* p = nullptr;
+        fe_status st = dev_alloc(c, &p, (size_t)slots * c->n * kTraceBytesPerParticle);
+        if (st != FE_OK) return st;
+        c->trace = p;
+        c->trace_cap = slots;
+    }
+    c->trace_slots = slots;
+    drop_graphs(c);
+    return FE_OK;
+}
+
+FE_API fe_status fe_debug_read_trace(fe_ctx* c, uint32_t slot, uint16_t* rows, float* out) {
+    if (!c || slot >= c->trace_slots) {
+        set_error("fe_debug_read_trace: no such slot (trace %u slots)", c ? c->trace_slots : 0u);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    const unsigned char* base = c->trace + (size_t)slot * c->n * kTraceBytesPerParticle;
+    if (rows)
+        FE_CUDA(cudaMemcpyAsync(rows, base, (size_t)c->n * 32, cudaMemcpyDeviceToHost,
+                                c->stream));
+    if (out)
+        FE_CUDA(cudaMemcpyAsync(out, base + (size_t)c->n * 32, (size_t)c->n * 8,
+                                cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
     return FE_OK;
 }
 

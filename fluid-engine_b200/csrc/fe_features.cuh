@@ -16,13 +16,19 @@
 //   2  div_i dt / (rho0 1e-3)  (the velocity-divergence term of the source)
 //   3  neighbour count / 32                4  last density kappa / scale_i
 //   5  last divergence kappa / scale_i     6  |v_i| dt / h
-//   7  sigma_i (this solve's source term)
-//   8..11  moments of order 1..4 of the neighbours' density residual,
-//          t_j = x / (1 + |x|) with x = 100 (rho_j / rho0 - 1), weighted by
-//          -grad_factor / (h r) (the list's kernel-gradient scale, >= 0):
-//          sum_j w_j t_j^k / sum_j w_j
+//   7..11  the 5 lowest moments (orders 1..5) of the neighbours' density
+//          residual, t_j = x / (1 + |x|) with x = 100 (rho_j / rho0 - 1),
+//          weighted by -grad_factor / (h r) (the list's kernel-gradient
+//          scale, >= 0): sum_j w_j t_j^k / sum_j w_j
 // ("last" = the most recent solve of that kind: before the divergence solve
-// the density kappa is the one just computed in this substep.)
+// the density kappa is the one just computed in this substep.)  The solve's
+// own source term in the same units is a fixed linear combination of
+// features 0 and 2 (-1000 f0 - f2 before the density solve, -f2 before the
+// divergence solve), so it is not a feature of its own.
+//
+// Every operation is IEEE single precision in the order written (no fast
+// division, no contraction), so the host oracle reproduces each feature and
+// its BF16 row bit for bit.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -48,17 +54,19 @@ __device__ __forceinline__ uint32_t sample_hash(uint32_t i, uint32_t seed) {
     return x;
 }
 
-// Running neighbourhood moments of the density residual.
+constexpr int kMoments = 5;
+
+// Running neighbourhood moments of the density residual (orders 1..5).
 struct Moments {
-    float w = 0.0f, m[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float w = 0.0f, m[kMoments] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     __device__ __forceinline__ void add(float g, float rho_j, float rho0) {
         float x = 100.0f * (rho_j / rho0 - 1.0f);
-        float t = __fdividef(x, 1.0f + fabsf(x));
+        float t = x / (1.0f + fabsf(x));
         float wj = -g;
         w += wj;
         float p = t;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kMoments; ++k) {
             m[k] += wj * p;
             p *= t;
         }
@@ -69,7 +77,7 @@ struct Moments {
 // (capture mode) for particle i before solve `which` (0 density, 1 divergence).
 __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
                                               const DevParams& P, uint32_t i, uint32_t scene,
-                                              int which, float src_i, float div_i, f3 v,
+                                              int which, float div_i, f3 v,
                                               const Moments& mo) {
     const float h = P.h, m = P.mass, dt = P.dt, rho0 = P.rho0;
     const float rho = B.rho[i], alpha = B.alpha[i];
@@ -85,9 +93,8 @@ __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
     f[4] = scale > 0.0f ? carry.x / scale : 0.0f;
     f[5] = scale > 0.0f ? carry.y / scale : 0.0f;
     f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * dt / h;
-    f[7] = sigma_of(src_i, dt, rho0);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) f[8 + k] = mo.w > 0.0f ? mo.m[k] / mo.w : 0.0f;
+    for (int k = 0; k < kMoments; ++k) f[7 + k] = mo.w > 0.0f ? mo.m[k] / mo.w : 0.0f;
 
     if (L.learned) {
         uint32_t packed[8];

@@ -423,7 +423,7 @@ __device__ __forceinline__ void density_source_body(const Bufs& B, const LearnAr
     B.src[i] = source;
     B.prs[i] = 0.0f;
     posb(B, i)->w = pressure_over_rho2(0.0f, rho_i);
-    if (kLearn) emit_features(B, L, P, i, s, 0, source, div, vi, mo);
+    if (kLearn) emit_features(B, L, P, i, s, 0, div, vi, mo);
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
@@ -467,7 +467,7 @@ __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
             [&](uint32_t, f3 rv, float g, float4, VelRho d) { term(rv, g, d.v, d.rho); });
     }
     B.src[i] = -div;
-    if (kLearn) emit_features(B, L, P, i, s, 1, -div, div, vi, mo);
+    if (kLearn) emit_features(B, L, P, i, s, 1, div, vi, mo);
 }
 
 __global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fixed) {

@@ -56,15 +56,22 @@ __global__ void __launch_bounds__(kBlock) k_warm_apply(Bufs B, LearnArgs L, int 
     const float y = L.out[2 * (size_t)i + which] * L.norm[26 + which] + L.norm[24 + which];
     const float4 carry = L.carry[i];
     const float base = which == 1 ? carry.x : 0.0f;
+    // Comparisons rather than fminf/fmaxf, so that no signed zero depends on
+    // how a maximum of -0 and +0 is taken: every value below is +0 or
+    // positive, and NaN becomes 0.
     float p1 = 0.0f;
     if (alpha > kEpsR && rho > kEpsR) {
         const float a_ii = -(P.dt / (rho * rho)) * alpha;
-        if (fabsf(a_ii) > 1e-20f) p1 = fmaxf((P.omega * B.src[i]) / a_ii, 0.0f);
+        if (fabsf(a_ii) > 1e-20f) {
+            const float q = (P.omega * B.src[i]) / a_ii;
+            p1 = q > 0.0f ? q : 0.0f;
+        }
     }
     const float d = p1 / P.omega;
     float p = B.nbr_count[i] < kMinNeighbours ? base : base + y * scale;
     p = p > 0.0f ? p : 0.0f;  // NaN -> 0; pressures are clamped at 0 as in pressure_update
-    p = fminf(p, fmaxf(d, carry.x));
+    const float bound = d > carry.x ? d : carry.x;
+    p = p < bound ? p : bound;
     B.prs[i] = p;
     posb(B, i)->w = pressure_over_rho2(p, rho);
 }

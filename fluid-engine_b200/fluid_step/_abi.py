@@ -330,6 +330,8 @@ SIGNATURES = {
     "fe_sort_noalloc_flags": (c_int, [c_void_p, c_void_p]),
     "fe_sort_flags": (c_int, [c_void_p, c_void_p]),
     "fe_debug_noalloc_wait_timeout": (c_int, [c_uint32, c_void_p]),
+    "fe_debug_trace_learned": (c_int, [c_void_p, c_uint32]),
+    "fe_debug_read_trace": (c_int, [c_void_p, c_uint32, c_void_p, c_void_p]),
     "fe_model_create": (c_int, [c_uint32, c_int, POINTER(c_void_p)]),
     "fe_model_destroy": (c_int, [c_void_p]),
     "fe_model_set_parameters": (c_int, [c_void_p, c_void_p, c_size_t]),

@@ -131,6 +131,22 @@ class GpuPhysicsData:
         return out
 
     # -- autotuning (fe_autotune) -------------------------------------------
+    # -- test hooks of the learned warm start --------------------------------
+    def trace_learned(self, slots: int) -> None:
+        """Record the network's input rows and outputs of the first `slots`
+        solves of every later frame (0: off)."""
+        check(self._lib, self._lib.fe_debug_trace_learned(self.handle, slots),
+              "fe_debug_trace_learned")
+
+    def read_trace(self, slot: int):
+        """(rows uint16[n][16], out float32[n][2]) of a solve of the last frame."""
+        rows = np.empty((self.count, 16), np.uint16)
+        out = np.empty((self.count, 2), np.float32)
+        check(self._lib, self._lib.fe_debug_read_trace(
+            self.handle, slot, rows.ctypes.data_as(ctypes.c_void_p),
+            out.ctypes.data_as(ctypes.c_void_p)), "fe_debug_read_trace")
+        return rows, out
+
     def autotune(self) -> _abi.FeTuneReport:
         r = _abi.FeTuneReport()
         check(self._lib, self._lib.fe_autotune(self.handle, ctypes.byref(r)), "fe_autotune")

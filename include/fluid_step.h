@@ -562,6 +562,19 @@ FE_API fe_status fe_capture_begin(fe_ctx* ctx, uint32_t capacity, uint32_t strid
 FE_API fe_status fe_capture_read(fe_ctx* ctx, float* x, float* y, uint32_t rows, uint32_t* count);
 FE_API fe_status fe_capture_end(fe_ctx* ctx);
 
+/* Test hook (no reference counterpart): with slots > 0, every later fe_step
+ * of a learned context records, for the first `slots` solves of the frame
+ * (slot 2k = the density solve of substep k, 2k + 1 = its divergence solve),
+ * the network's input rows as the source passes wrote them and its output
+ * as the warm start read it.  0 turns the record off.  Frame graphs are
+ * recorded again.  Lets a test check the features against an independent
+ * restatement and feed the same network outputs to it. */
+FE_API fe_status fe_debug_trace_learned(fe_ctx* ctx, uint32_t slots);
+/* Slot `slot` of the last fe_step: rows[n][16] BF16 bit patterns (features
+ * 0..11 standardised, 12..15 zero), out[n][2] the network's standardised
+ * outputs.  Either may be NULL.  Synchronous. */
+FE_API fe_status fe_debug_read_trace(fe_ctx* ctx, uint32_t slot, uint16_t* rows, float* out);
+
 /* Radix sort that allocates nothing.  No counterpart in the reference: it is
  * for callers that cannot let a library allocate device memory — a frame
  * loop that must not stall (cudaMalloc/cudaFree synchronise the device),

@@ -350,12 +350,42 @@ struct Base {
     virtual int download(int field, void* dst, size_t bytes) const = 0;
     virtual int download_f64(int field, double* dst, size_t count) const = 0;
     virtual int upload(int field, const void* src, size_t bytes) = 0;
+
+    // Learned warm start (no reference counterpart; restates
+    // fe_features.cuh, fe_learned.cu and the carry through reorder of the
+    // CUDA library).  The network itself is not restated: its per-particle
+    // outputs for each solve of the next frame are given (net_out), the
+    // features it was fed are kept (rows) for comparison.
+    bool learned = false;
+    float norm[28] = {};
+    uint32_t net_slots = 0;        // solves with outputs given for the next frame
+    std::vector<float> net_out;    // [slot][n][2], standardised outputs
+    std::vector<uint16_t> rows;    // [slot][n][16], BF16 network inputs of the last frame
+    uint32_t cur_substep = 0;      // substep of the frame being computed
+    bool net_missing = false;      // a solve had no given outputs
+    virtual void warm_apply(int which) = 0;
+    virtual void after_solve(int which) = 0;
 };
+
+// __float2bfloat16_rn: round to nearest even; NaN -> the canonical 0x7FFF.
+inline uint16_t bf16_rn(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7FFFFFFFu) > 0x7F800000u) return 0x7FFFu;
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
 
 template <class R>
 struct State : Base {
     std::vector<V4<R>> pos_a, pos_b, vel_a, vel_b, acc;
     std::vector<R> rho, alpha, src, prs, prs_tmp;
+    // learned warm start: carry[i] = {last density kappa, last divergence
+    // kappa, -, -} travelling with particle i; neighbours with r > 1e-6 per
+    // particle from the last density_alpha (duplicates of a doubly visited
+    // bucket counted twice, like the walk)
+    std::vector<V4<R>> carry, carry_tmp;
+    std::vector<uint32_t> nbr_count;
 
     R h() const { return (R)p.smoothing_radius; }
     R mass() const { return (R)p.particle_mass; }
@@ -438,8 +468,10 @@ struct State : Base {
             pos_b[i] = pos_a[s];
             vel_b[i] = vel_a[s];
             if (fixed) prs_tmp[i] = prs[s];
+            if (learned) carry_tmp[i] = carry[s];
         }
         if (fixed) std::swap(prs, prs_tmp);
+        if (learned) std::swap(carry, carry_tmp);
         return 0;
     }
 
@@ -451,6 +483,7 @@ struct State : Base {
             uint32_t i = (uint32_t)ii;
             R density = 0, sum_grad_sq = 0;
             V3<R> grad_sum{0, 0, 0};
+            uint32_t cnt = 0;
             for_neighbors(i, [&](uint32_t, V3<R> rv, R r2) {
                 R r = std::sqrt(r2);
                 R w = kernel_w(r, hh);
@@ -460,8 +493,10 @@ struct State : Base {
                     V3<R> mg = scale(m, grad);
                     grad_sum = add(grad_sum, mg);
                     sum_grad_sq += dot(mg, mg);
+                    ++cnt;
                 }
             });
+            nbr_count[i] = cnt;
             rho[i] = density;
             R a = sum_grad_sq + dot(grad_sum, grad_sum);
             alpha[i] = a > K<R>::eps_r() ? a : R(0);
@@ -501,40 +536,148 @@ struct State : Base {
             uint32_t i = (uint32_t)ii;
             V3<R> vi = xyz(vel_a[i]);
             R div = 0;
+            Moments mo;
             for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
                 R r = std::sqrt(r2);
                 if (r > K<R>::eps_r()) {
-                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                    R g = kernel_grad_scale(r, hh);
+                    V3<R> grad = scale(g, rv);
                     V3<R> vd = sub(vi, xyz(vel_a[j]));
                     div += m * dot(vd, grad);
+                    if (learned) mo.add(g, rho[j], rho0);
                 }
             });
             R source = 0;
             if (d > K<R>::eps_r()) source = ((rho0 - rho[i]) / d) - div;
             src[i] = source;
             prs[i] = 0;
+            if (learned) emit_row(i, 0, div, vi, mo);
+        }
+    }
+
+    // ---- learned warm start ------------------------------------------------
+    // Moments of order 1..5 of the neighbours' density residual
+    // (fe_features.cuh, Moments::add): t = x / (1 + |x|), x = 100 (rho_j /
+    // rho0 - 1), weighted by -grad_factor / (h r).
+    struct Moments {
+        R w = 0, m[5] = {0, 0, 0, 0, 0};
+        void add(R g, R rho_j, R rho0) {
+            R x = R(100) * (rho_j / rho0 - R(1));
+            R t = x / (R(1) + std::fabs(x));
+            R wj = -g;
+            w += wj;
+            R pw = t;
+            for (int k = 0; k < 5; ++k) {
+                m[k] += wj * pw;
+                pw *= t;
+            }
+        }
+    };
+
+    // kappa_scale (fe_features.cuh): rho^2 / (dt alpha) * (rho0 1e-3 / dt).
+    R kappa_scale(R rho_i, R al, R d, R rho0) const {
+        R eps = K<R>::eps_r();
+        if (!(al > eps && rho_i > eps && d > eps)) return R(0);
+        return (rho_i * rho_i / (d * al)) * (rho0 * R(1e-3f) / d);
+    }
+
+    // emit_features (fe_features.cuh): the 12 features of particle i before
+    // solve `which`, standardised with the model's statistics, as the BF16
+    // row the network reads.
+    void emit_row(uint32_t i, int which, R div, V3<R> v, const Moments& mo) {
+        uint32_t slot = 2u * cur_substep + (uint32_t)which;
+        if (slot >= net_slots) return;
+        R hh = h(), m = mass(), d = dt(), rho0 = (R)p.target_density;
+        R rho_i = rho[i], al = alpha[i];
+        R sc = kappa_scale(rho_i, al, d, rho0);
+        R f[12];
+        f[0] = rho_i / rho0 - R(1);
+        R h2 = hh * hh, h4 = h2 * h2;
+        f[1] = al * (h4 * h4) / (m * m);
+        f[2] = div * d / (rho0 * R(1e-3f));
+        uint32_t cnt = nbr_count[i];
+        f[3] = (R)(cnt < 64u ? cnt : 64u) / R(32);
+        f[4] = sc > R(0) ? carry[i].x / sc : R(0);
+        f[5] = sc > R(0) ? carry[i].y / sc : R(0);
+        f[6] = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z) * d / hh;
+        for (int k = 0; k < 5; ++k) f[7 + k] = mo.w > R(0) ? mo.m[k] / mo.w : R(0);
+        uint16_t* row = rows.data() + ((size_t)slot * n + i) * 16;
+        for (int k = 0; k < 16; ++k) {
+            R a = k < 12 ? (f[k] - (R)norm[k]) / (R)norm[12 + k] : R(0);
+            row[k] = bf16_rn((float)a);
+        }
+    }
+
+    // k_warm_apply (fe_learned.cu): the solve's start from the network's
+    // output, clamped to [0, max(d_i, carried density kappa)]; particles with
+    // fewer than 16 neighbours keep the plain start.
+    void warm_apply(int which) override {
+        uint32_t slot = 2u * cur_substep + (uint32_t)which;
+        if (slot >= net_slots) {
+            net_missing = true;
+            return;
+        }
+        const float* out = net_out.data() + (size_t)slot * n * 2;
+        R d = dt(), omega = (R)p.relax_factor, rho0 = (R)p.target_density;
+        R eps = K<R>::eps_r();
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            uint32_t i = (uint32_t)ii;
+            R rho_i = rho[i], al = alpha[i];
+            R sc = kappa_scale(rho_i, al, d, rho0);
+            R y = (R)out[2 * (size_t)i + which] * (R)norm[26 + which] + (R)norm[24 + which];
+            R base = which == 1 ? carry[i].x : R(0);
+            R p1 = 0;
+            if (al > eps && rho_i > eps) {
+                R a_ii = -(d / (rho_i * rho_i)) * al;
+                if (std::fabs(a_ii) > R(1e-20)) {
+                    R q = (omega * src[i]) / a_ii;
+                    p1 = q > R(0) ? q : R(0);
+                }
+            }
+            R dd = p1 / omega;
+            R pr = nbr_count[i] < 16u ? base : base + y * sc;
+            pr = pr > R(0) ? pr : R(0);
+            R bound = dd > carry[i].x ? dd : carry[i].x;
+            prs[i] = pr < bound ? pr : bound;
+        }
+    }
+
+    // after_solve_particle (fe_features.cuh): the solve's final pressure
+    // becomes the particle's last kappa of that kind.
+    void after_solve(int which) override {
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+            if (which == 0)
+                carry[ii].x = prs[ii];
+            else
+                carry[ii].y = prs[ii];
         }
     }
 
     // divergence_source_term.comp:14-61 (velocities = velocity_a in
     // REFERENCE mode, divergence_source_term.rs:47).
     void divergence_source() override {
-        R m = mass(), hh = h();
+        R m = mass(), hh = h(), rho0 = (R)p.target_density;
         const std::vector<V4<R>>& vel = vel_div();
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
         for (long long ii = 0; ii < (long long)n; ++ii) {
             uint32_t i = (uint32_t)ii;
             V3<R> vi = xyz(vel[i]);
             R div = 0;
+            Moments mo;
             for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
                 R r = std::sqrt(r2);
                 if (r > K<R>::eps_r()) {
-                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
+                    R g = kernel_grad_scale(r, hh);
+                    V3<R> grad = scale(g, rv);
                     V3<R> vd = sub(vi, xyz(vel[j]));
                     div += m * dot(vd, grad);
+                    if (learned) mo.add(g, rho[j], rho0);
                 }
             });
             src[i] = -div;
+            if (learned) emit_row(i, 1, div, vi, mo);
         }
     }
 
@@ -773,6 +916,9 @@ Base* make_state(const fe_params* params, uint32_t n, const float* pos, const fl
     s->src.assign(n, 0);
     s->prs.assign(n, 0);
     s->prs_tmp.assign(n, 0);
+    s->carry.assign(n, {0, 0, 0, 0});
+    s->carry_tmp.assign(n, {0, 0, 0, 0});
+    s->nbr_count.assign(n, 0);
     s->ekey.assign(s->T, 0);
     s->eidx.assign(s->T, 0);
     s->grid_start.assign(s->T, 0);
@@ -863,6 +1009,7 @@ void substep(Base* s, fe_stats* acc_stats, bool* cap_hit) {
     double r;
     s->viscosity();
     s->density_source();
+    if (s->learned) s->warm_apply(0);
     double rm = 0.0;
     uint32_t kr = solve(s, false, &r, cap_hit, &rm);
     acc_stats->density_residual_max = rm;
@@ -870,15 +1017,18 @@ void substep(Base* s, fe_stats* acc_stats, bool* cap_hit) {
     acc_stats->total_density_iterations += kr;
     acc_stats->density_residual = r;
     s->pressure_integration();
+    if (s->learned) s->after_solve(0);
     s->neighbor_search();
     s->density_alpha();
     s->divergence_source();
+    if (s->learned) s->warm_apply(1);
     uint32_t kd = solve(s, true, &r, cap_hit, &rm);
     acc_stats->divergence_residual_max = rm;
     acc_stats->divergence_iterations = kd;
     acc_stats->total_divergence_iterations += kd;
     acc_stats->divergence_residual = r;
     s->divergence_integration();
+    if (s->learned) s->after_solve(1);
 }
 
 void fill_stats(Base* s, fe_stats* out) {
@@ -966,7 +1116,13 @@ int fo_step(fo_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {
     fe_stats st = s->last;
     st.density_iterations = st.divergence_iterations = 0;
     bool cap_hit = false;
-    for (uint32_t k = 0; k < n_substeps; ++k) substep(s, &st, &cap_hit);
+    if (s->learned) s->rows.assign((size_t)s->net_slots * s->n * 16, 0);
+    for (uint32_t k = 0; k < n_substeps; ++k) {
+        s->cur_substep = k;
+        substep(s, &st, &cap_hit);
+    }
+    s->cur_substep = 0;
+    if (s->learned) s->net_slots = 0;  // outputs are given per frame
     s->stats_pass();
     fill_stats(s, &st);
     st.substeps = n_substeps;
@@ -975,6 +1131,35 @@ int fo_step(fo_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {
     if (out) *out = st;
     return 0;
 }
+
+int fo_set_learned(fo_ctx* c, const float* norm28) {
+    if (!c) return FE_ERR_INVALID_ARGUMENT;
+    Base* s = c->s;
+    s->learned = norm28 != nullptr;
+    if (norm28) std::memcpy(s->norm, norm28, sizeof s->norm);
+    s->net_slots = 0;
+    return 0;
+}
+
+int fo_set_network_outputs(fo_ctx* c, uint32_t slots, const float* out) {
+    if (!c || !c->s->learned || (slots && !out)) return FE_ERR_INVALID_ARGUMENT;
+    Base* s = c->s;
+    s->net_out.assign(out, out + (size_t)slots * s->n * 2);
+    s->net_slots = slots;
+    s->net_missing = false;
+    return 0;
+}
+
+int fo_get_feature_rows(const fo_ctx* c, uint32_t slot, uint16_t* rows) {
+    if (!c || !rows) return FE_ERR_INVALID_ARGUMENT;
+    const Base* s = c->s;
+    size_t per = (size_t)s->n * 16;
+    if ((size_t)(slot + 1) * per > s->rows.size()) return FE_ERR_INVALID_ARGUMENT;
+    std::memcpy(rows, s->rows.data() + slot * per, per * sizeof(uint16_t));
+    return 0;
+}
+
+int fo_learned_missing_outputs(const fo_ctx* c) { return c && c->s->net_missing ? 1 : 0; }
 
 int fo_download(const fo_ctx* c, int field, void* dst, size_t bytes) {
     if (!c) return FE_ERR_INVALID_ARGUMENT;

@@ -91,6 +91,21 @@ void fo_raymarch(const uint32_t* grid, int rx, int ry, int rz, const float* sky4
                  int sky_h, const float* inv_view_proj, const float* cam_pos,
                  const float* box_min, const float* box_max, int width, int height, float* out);
 
+/* Learned warm start (restates the CUDA library's fe_features.cuh and
+ * fe_learned.cu; no reference counterpart).  fo_set_learned(norm28) turns
+ * it on with the model's standardisation (x mean[12], x std[12], y mean[2],
+ * y std[2]); NULL turns it off.  The network is not restated: before each
+ * fo_step, fo_set_network_outputs gives its standardised outputs out[slot]
+ * [n][2] for the frame's first `slots` solves (slot 2k = density solve of
+ * substep k, 2k + 1 = divergence solve); after it, fo_get_feature_rows
+ * returns the BF16 rows rows[n][16] the source passes computed for a slot.
+ * fo_learned_missing_outputs: the last fo_step reached a solve without
+ * given outputs (its start was left as without the network). */
+int fo_set_learned(fo_ctx* ctx, const float* norm28);
+int fo_set_network_outputs(fo_ctx* ctx, uint32_t slots, const float* out);
+int fo_get_feature_rows(const fo_ctx* ctx, uint32_t slot, uint16_t* rows);
+int fo_learned_missing_outputs(const fo_ctx* ctx);
+
 int fo_set_threads(int threads);
 int fo_get_threads(void);
 

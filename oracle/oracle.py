@@ -56,6 +56,10 @@ def lib():
             "fo_raymarch": (None, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
                                    c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                    c_void_p]),
+            "fo_set_learned": (c_int, [c_void_p, c_void_p]),
+            "fo_set_network_outputs": (c_int, [c_void_p, c_uint32, c_void_p]),
+            "fo_get_feature_rows": (c_int, [c_void_p, c_uint32, c_void_p]),
+            "fo_learned_missing_outputs": (c_int, [c_void_p]),
             "fo_set_threads": (c_int, [c_int]),
             "fo_get_threads": (c_int, []),
         }
@@ -147,6 +151,39 @@ class Oracle:
         if rc:
             raise RuntimeError(f"oracle download {field}: {rc}")
         return out.reshape(count, width) if width == 4 else out
+
+    # -- learned warm start (the network's outputs are given, not computed) --
+    def set_learned(self, norm) -> None:
+        """Turns the warm start on with the model's standardisation (28
+        floats: x mean[12], x std[12], y mean[2], y std[2]); None: off."""
+        if norm is None:
+            self._norm = None
+            rc = lib().fo_set_learned(self.h, None)
+        else:
+            self._norm = np.ascontiguousarray(norm[:28], dtype=np.float32)
+            rc = lib().fo_set_learned(self.h, _ptr(self._norm))
+        if rc:
+            raise RuntimeError(f"oracle set_learned: {rc}")
+
+    def set_network_outputs(self, outs) -> None:
+        """outs[slot][n][2]: the network's standardised outputs for the
+        next frame's solves (slot 2k density, 2k + 1 divergence)."""
+        a = np.ascontiguousarray(outs, dtype=np.float32).reshape(-1, self.n, 2)
+        self._outs = a
+        rc = lib().fo_set_network_outputs(self.h, a.shape[0], _ptr(a))
+        if rc:
+            raise RuntimeError(f"oracle set_network_outputs: {rc}")
+
+    def feature_rows(self, slot: int) -> np.ndarray:
+        """uint16[n][16]: the BF16 network inputs of a solve of the last frame."""
+        out = np.empty((self.n, 16), np.uint16)
+        rc = lib().fo_get_feature_rows(self.h, slot, _ptr(out))
+        if rc:
+            raise RuntimeError(f"oracle feature_rows({slot}): {rc}")
+        return out
+
+    def missing_network_outputs(self) -> bool:
+        return bool(lib().fo_learned_missing_outputs(self.h))
 
     def upload(self, field: int, data: np.ndarray):
         dt = np.uint32 if field in _abi.UINT_FIELDS else np.float32

@@ -308,3 +308,26 @@ def test_nan_state_reports_non_finite():
     with pytest.raises(_abi.FluidStepError) as e:
         sim.step(1)
     assert e.value.status == _abi.FE_ERR_NON_FINITE
+
+
+# --------------------------------------------------------------------------
+# Benchmarked sizes: the 2^20-slot hash table, bucket collisions (Q3) and
+# neighbour-list overflow at scale
+# --------------------------------------------------------------------------
+def test_frames_bit_exact_1m_tolerance(oracle_mod):
+    """The benchmarked 1M dam break (FIXED mode, Jacobi to 0.1 % density
+    and divergence error) with a seeded velocity field, so that the solves
+    iterate: 2 frames, every field and every stats word."""
+    w = scene.workload("dam_break_1m")
+    pos = w.positions()
+    vel = np.random.default_rng(3).normal(0, 0.3, pos.shape).astype(np.float32)
+    sim, orc, st = _run_frames(oracle_mod, w.params, pos, frames=2, vel=vel)
+    assert sim.data.table_size == 1 << 20
+    assert st.density_iterations >= 1 and st.divergence_iterations >= 1
+
+
+def test_frames_bit_exact_262k_adaptive_cfl(oracle_mod):
+    """The 262k dam break with adaptive CFL and the tolerance solver: 3
+    frames (dt changes every frame on the device)."""
+    w = scene.workload("dam_break_256k")
+    _run_frames(oracle_mod, w.params, w.positions(), frames=3)
