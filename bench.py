@@ -290,21 +290,37 @@ def measure_arm(args, w, params, model, world, local):
     iters_v = (st.total_divergence_iterations - it0[1]) / args.steps
     dev_ms_max = reduce_max(dev_ms, world)
 
-    # e2e through the C ABI: parameter block in (sync_with_scene), stats and
-    # the render copy of position_a out, every frame.
+    # e2e through the C ABI as a host application drives it: every frame the
+    # parameter block goes in (sync_with_scene), the frame runs, its stats
+    # come back (the next dt) and its positions are copied out for the
+    # renderer.  The positions' copy (fe_download_async into page-locked
+    # memory, two buffers) overlaps the next frame; the host waits for frame
+    # k's positions after launching frame k+1, and for the last frame's before
+    # the clock stops.
     p = _abi.copy_params(sim.data.current_params())
-    pos_host = np.empty((n, 4), np.float32)
+    pinned = [torch.empty((n, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    pos_host = [t.numpy() for t in pinned]
     stats_host = _abi.FeStats()
+    ticket = ctypes.c_uint64()
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    prev = 0
+    for k in range(args.steps):
         lib.fe_set_params(h, ctypes.byref(p))
         lib.fe_step(h, 1, step_flags, None)
         lib.fe_read_stats(h, ctypes.byref(stats_host))
-        lib.fe_download(h, _abi.FE_FIELD_POSITION_A, pos_host.ctypes.data_as(ctypes.c_void_p),
-                        pos_host.nbytes)
+        buf = pos_host[k % 2]
+        rc = lib.fe_download_async(h, _abi.FE_FIELD_POSITION_A,
+                                   buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes,
+                                   ctypes.byref(ticket))
+        if rc:
+            raise RuntimeError(f"fe_download_async failed: {rc}")
+        if prev:
+            lib.fe_download_wait(h, prev)
+        prev = ticket.value
         p.dt = stats_host.dt
+    lib.fe_download_wait(h, prev)
     e2e_s = reduce_max(time.perf_counter() - t0, world)
 
     kern = {}
@@ -684,7 +700,8 @@ def run_gpu(args) -> None:
             "e2e": {"value": head["e2e"], "unit": "particle-steps/s",
                     "h2d_bytes_per_step": ctypes.sizeof(_abi.FeParams),
                     "d2h_bytes_per_step": n * 16 + ctypes.sizeof(_abi.FeStats),
-                    "path": "fe_set_params + fe_step + fe_read_stats + fe_download(position_a)"},
+                    "path": "fe_set_params + fe_step + fe_read_stats + fe_download_async("
+                            "position_a, page-locked) overlapping the next frame"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,

@@ -321,6 +321,16 @@ struct fe_ctx {
     size_t image_cap = 0;
     int image_w = 0, image_h = 0;
 
+    // fe_download_async: two device snapshots, the copy stream, and which
+    // ticket each snapshot slot serves (0: none)
+    cudaStream_t copy_stream = nullptr;
+    void* snap[2] = {nullptr, nullptr};
+    size_t snap_cap = 0;
+    cudaEvent_t snap_ready[2] = {nullptr, nullptr};
+    cudaEvent_t copy_done[2] = {nullptr, nullptr};
+    uint64_t tickets = 0;
+    uint64_t slot_ticket[2] = {0, 0};
+
     // tuned shapes (fe_autotune / fe_set_tuning)
     RadixConfig radix_cfg = kRadixDefault;
     int mlp_ctas = mlp::kInferDefaultCtasPerSm;
@@ -377,6 +387,14 @@ void release(fe_ctx* c) {
     c->allocations.clear();
     if (c->h_state) cudaFreeHost(c->h_state);
     if (c->h_global) cudaFreeHost(c->h_global);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (c->snap_ready[k]) cudaEventDestroy(c->snap_ready[k]);
+        if (c->copy_done[k]) cudaEventDestroy(c->copy_done[k]);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -1207,6 +1225,90 @@ fe_status fe_download(fe_ctx* c, fe_field f, void* dst, size_t bytes) {
         float* v = static_cast<float*>(dst);
         for (uint32_t i = 0; i < c->n; ++i) v[4 * i + 3] = 0.0f;
     }
+    return FE_OK;
+}
+
+// The reference's w of a float4 field whose device copy keeps other data
+// in w: position_b.w = 1 (the copied position_a.w), the velocities' w = 0.
+bool field_fixed_w(fe_field f, float* w) {
+    if (f == FE_FIELD_POSITION_B) {
+        *w = 1.0f;
+        return true;
+    }
+    if (f == FE_FIELD_VELOCITY_A || f == FE_FIELD_VELOCITY_B) {
+        *w = 0.0f;
+        return true;
+    }
+    return false;
+}
+
+fe_status fe_download_async(fe_ctx* c, fe_field f, void* dst, size_t bytes, uint64_t* ticket) {
+    if (!c || !dst || !ticket) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    void* d;
+    size_t elem, pitch;
+    size_t need = field_bytes(c, f, &d, &elem, &pitch);
+    if (need == 0 || bytes != need) {
+        set_error("field %d: expected %zu bytes, got %zu", (int)f, need, bytes);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    if (!c->copy_stream) {
+        FE_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            FE_CUDA(cudaEventCreateWithFlags(&c->snap_ready[k], cudaEventDisableTiming));
+            FE_CUDA(cudaEventCreateWithFlags(&c->copy_done[k], cudaEventDisableTiming));
+        }
+    }
+    if (need > c->snap_cap) {
+        // earlier snapshots may still be copied out of the old buffers
+        FE_CUDA(cudaStreamSynchronize(c->copy_stream));
+        unsigned char *a = nullptr, *b = nullptr;
+        fe_status st;
+        if ((st = dev_alloc(c, &a, need)) != FE_OK || (st = dev_alloc(c, &b, need)) != FE_OK)
+            return st;
+        c->snap[0] = a;
+        c->snap[1] = b;
+        c->snap_cap = need;
+        c->slot_ticket[0] = c->slot_ticket[1] = 0;
+    }
+    const uint64_t t = ++c->tickets;
+    const int slot = (int)(t & 1u);
+    // the slot's previous copy must have left the snapshot before it is
+    // overwritten
+    if (c->slot_ticket[slot]) FE_CUDA(cudaStreamWaitEvent(c->stream, c->copy_done[slot], 0));
+    float w = 0.0f;
+    const bool fix_w = field_fixed_w(f, &w);
+    if (elem == 16) {
+        Recorder R = eager(c);
+        REC(R.k(k_snapshot4, flat_grid((uint32_t)(need / 16)), dim3(kBlock),
+                static_cast<float4*>(c->snap[slot]), static_cast<const float4*>(d),
+                (uint32_t)(pitch / 16), (uint32_t)(need / 16), fix_w ? 1 : 0, w));
+    } else {
+        FE_CUDA(cudaMemcpy2DAsync(c->snap[slot], elem, d, pitch, elem, need / elem,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+    }
+    FE_CUDA(cudaEventRecord(c->snap_ready[slot], c->stream));
+    FE_CUDA(cudaStreamWaitEvent(c->copy_stream, c->snap_ready[slot], 0));
+    FE_CUDA(cudaMemcpyAsync(dst, c->snap[slot], need, cudaMemcpyDeviceToHost, c->copy_stream));
+    FE_CUDA(cudaEventRecord(c->copy_done[slot], c->copy_stream));
+    c->slot_ticket[slot] = t;
+    *ticket = t;
+    return FE_OK;
+}
+
+fe_status fe_download_wait(fe_ctx* c, uint64_t ticket) {
+    if (!c || ticket == 0 || ticket > c->tickets) {
+        set_error("fe_download_wait: unknown ticket %llu", (unsigned long long)ticket);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    // A slot serves tickets in increasing order, and each copy out of a slot
+    // follows the one before it: waiting for the slot's latest copy covers
+    // this ticket as well.
+    FE_CUDA(cudaEventSynchronize(c->copy_done[ticket & 1u]));
     return FE_OK;
 }
 

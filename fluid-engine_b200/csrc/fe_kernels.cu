@@ -121,6 +121,19 @@ __global__ void __launch_bounds__(kBlock) k_take_pressure_carry(Bufs B, LearnArg
     take_pressure_body<true>(B, L);
 }
 
+// Snapshot of a float4 field for fe_download_async: element i of a field
+// whose elements lie `stride` float4 apart, with w replaced by `w` when
+// fix_w (the reference's w of that field; the device keeps other data there).
+__global__ void __launch_bounds__(kBlock) k_snapshot4(float4* dst, const float4* src,
+                                                      uint32_t stride, uint32_t n, int fix_w,
+                                                      float w) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = src[(size_t)i * stride];
+    if (fix_w) v.w = w;
+    dst[i] = v;
+}
+
 // pr = p / rho^2 and both velocities' w = rho for all particles (after a
 // host upload of p, rho, position_b or a velocity).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {

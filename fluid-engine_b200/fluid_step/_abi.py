@@ -306,6 +306,8 @@ SIGNATURES = {
     "fe_synchronize": (c_int, [CTX]),
     "fe_upload": (c_int, [CTX, c_int, c_void_p, c_size_t]),
     "fe_download": (c_int, [CTX, c_int, c_void_p, c_size_t]),
+    "fe_download_async": (c_int, [CTX, c_int, c_void_p, c_size_t, POINTER(ctypes.c_uint64)]),
+    "fe_download_wait": (c_int, [CTX, ctypes.c_uint64]),
     "fe_neighbor_search": (c_int, [CTX]),
     "fe_density_alpha": (c_int, [CTX]),
     "fe_viscosity": (c_int, [CTX]),

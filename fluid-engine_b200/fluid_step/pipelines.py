@@ -74,6 +74,19 @@ class GpuPhysicsData:
               "fe_download")
         return out.reshape(count, 4) if width == 4 else out
 
+    def download_async(self, field: int, out: np.ndarray) -> int:
+        """Starts copying `field` into `out` (a C-contiguous array of the
+        field's size, ideally in page-locked memory) without waiting; returns
+        the ticket for download_wait.  `out` must stay alive until then."""
+        t = ctypes.c_uint64()
+        check(self._lib, self._lib.fe_download_async(
+            self.handle, field, out.ctypes.data_as(ctypes.c_void_p), out.nbytes,
+            ctypes.byref(t)), "fe_download_async")
+        return int(t.value)
+
+    def download_wait(self, ticket: int) -> None:
+        check(self._lib, self._lib.fe_download_wait(self.handle, ticket), "fe_download_wait")
+
     def upload(self, field: int, data) -> None:
         dt = np.uint32 if field in _abi.UINT_FIELDS else np.float32
         a = np.ascontiguousarray(data, dtype=dt)

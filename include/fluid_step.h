@@ -289,6 +289,18 @@ FE_API fe_status fe_synchronize(fe_ctx* ctx);
  * stream; download completes before returning. */
 FE_API fe_status fe_upload(fe_ctx* ctx, fe_field field, const void* src, size_t bytes);
 FE_API fe_status fe_download(fe_ctx* ctx, fe_field field, void* dst, size_t bytes);
+/* Download without waiting (the render copy of `Renderer::step`,
+ * renderer/mod.rs:347-355, moved off the frame's critical path).  The field
+ * is snapshotted on the device in the context's stream order, so fe_step
+ * calls made right after see no change, and copied to `dst` on a second
+ * stream while later work runs; *ticket identifies the copy.  `dst` must stay
+ * valid, and should be page-locked (cudaHostAlloc, cudaHostRegister) for the
+ * copy to overlap; it holds the field, with the reference's w as fe_download
+ * gives it, once fe_download_wait(ticket) returns.  Two snapshots rotate:
+ * a third fe_download_async waits, on the device, for the copy of the first. */
+FE_API fe_status fe_download_async(fe_ctx* ctx, fe_field field, void* dst, size_t bytes,
+                                   uint64_t* ticket);
+FE_API fe_status fe_download_wait(fe_ctx* ctx, uint64_t ticket);
 
 /* ------------------------------------------------------------------------- */
 /* Stage entry points: one per `ComputeStep::execute`                         */
