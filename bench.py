@@ -270,6 +270,9 @@ def measure_arm(args, w, params, model, world, local):
     step_flags = _abi.FE_STEP_NO_GRAPH if args.eager else 0
     for _ in range(args.warmup):
         st = sim.step(1, step_flags)
+    # the state at the start of the timed window: the e2e run below replays
+    # the same K frames from it (fe_state_import restores it bit for bit)
+    window_start = sim.data.export_state()
     barrier(world)
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -290,13 +293,16 @@ def measure_arm(args, w, params, model, world, local):
     iters_v = (st.total_divergence_iterations - it0[1]) / args.steps
     dev_ms_max = reduce_max(dev_ms, world)
 
-    # e2e through the C ABI as a host application drives it: every frame the
+    # e2e through the C ABI as a host application drives it, over the same K
+    # frames as the device-timed window (replayed from its start): every frame the
     # parameter block goes in (sync_with_scene), the frame runs, its stats
     # come back (the next dt) and its positions are copied out for the
     # renderer.  The positions' copy (fe_download_async into page-locked
     # memory, two buffers) overlaps the next frame; the host waits for frame
     # k's positions after launching frame k+1, and for the last frame's before
     # the clock stops.
+    sim.data.import_state(window_start)
+    del window_start
     p = _abi.copy_params(sim.data.current_params())
     pinned = [torch.empty((n, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
     pos_host = [t.numpy() for t in pinned]
@@ -354,43 +360,82 @@ def measure_arm(args, w, params, model, world, local):
             "tuning": tune_report}
 
 
-def sort_benchmark(lib):
-    """Isolated radix sort: 2^22 uniform random u32 keys with a u32 payload,
-    median of 15 after 3 warm-ups (the reference's protocol, sorter.rs:708-709)."""
+def _time_sorts(fn, prep=None, reps: int = 15, warm: int = 3) -> float:
+    """Median CUDA-event time (ms) of fn() over `reps` runs after `warm`;
+    prep() runs before each, outside the timed region."""
+    import torch
+    cs = torch.cuda.current_stream()
+    times = []
+    for it in range(warm + reps):
+        if prep:
+            prep()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        fn()
+        b.record(cs)
+        b.synchronize()
+        if it >= warm:
+            times.append(a.elapsed_time(b))
+    return statistics.median(times)
+
+
+def sort_benchmark(lib, peak_gbs: float):
+    """Isolated radix sort over N = 2^15 .. 2^22 uniform random u32 keys with
+    a u32 payload (the index), median of 15 after 3 warm-ups per N (the
+    reference's protocol, sorter.rs:695-709).  The autotuner picks the radix
+    shape per size class first.  Beside it, torch.sort(stable=True) of the
+    same keys as int32 (CUB's radix sort with int64 indices as the payload)
+    as a library reference point.  Roofline: 4 B key + 16 B per pass moved
+    (read and write of key and value) over 4 passes = 68 B per key."""
     import torch
 
     from fluid_step import _abi
-    sort_n = 1 << 22
-    rng = np.random.default_rng(0)
-    kd = torch.from_numpy(rng.integers(0, 2**32, sort_n, dtype=np.uint64).astype(np.uint32)
-                          .view(np.int32)).cuda()
-    vd = torch.arange(sort_n, dtype=torch.int32, device="cuda")
-    # The autotuner times every radix shape on these keys first; fe_sort_pairs
-    # then uses its choice for this size class.
-    rep = _abi.FeTuneReport()
-    _abi.check(lib, lib.fe_autotune_sort(ctypes.c_void_p(kd.data_ptr()),
-                                         ctypes.c_void_p(vd.data_ptr()), sort_n, 32,
-                                         ctypes.byref(rep)), "fe_autotune_sort")
-    k2, v2 = kd.clone(), vd.clone()
     cs = torch.cuda.current_stream()
-    times = []
-    for it in range(18):
-        k2.copy_(kd)
-        v2.copy_(vd)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(cs)
-        lib.fe_sort_pairs(ctypes.c_void_p(k2.data_ptr()), ctypes.c_void_p(v2.data_ptr()), sort_n, 32,
-                          _abi.FE_SORT_RADIX, ctypes.c_void_p(cs.cuda_stream))
-        b.record(cs)
-        b.synchronize()
-        if it >= 3:
-            times.append(a.elapsed_time(b))
-    ms = statistics.median(times)
-    ch = rep.chosen
-    passes = -(-32 // ch.radix_digit_bits)
-    return {"n": sort_n, "ms": ms, "keys_per_s": sort_n / (ms / 1e3),
+    sweep = []
+    chosen = None
+    for log_n in range(15, 23):
+        n = 1 << log_n
+        rng = np.random.default_rng(log_n)
+        kd = torch.from_numpy(rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+                              .view(np.int32)).cuda()
+        vd = torch.arange(n, dtype=torch.int32, device="cuda")
+        rep = _abi.FeTuneReport()
+        _abi.check(lib, lib.fe_autotune_sort(ctypes.c_void_p(kd.data_ptr()),
+                                             ctypes.c_void_p(vd.data_ptr()), n, 32,
+                                             ctypes.byref(rep)), "fe_autotune_sort")
+        k2, v2 = kd.clone(), vd.clone()
+
+        def fresh():
+            k2.copy_(kd)
+            v2.copy_(vd)
+
+        def ours():
+            lib.fe_sort_pairs(ctypes.c_void_p(k2.data_ptr()), ctypes.c_void_p(v2.data_ptr()), n,
+                              32, _abi.FE_SORT_RADIX, ctypes.c_void_p(cs.cuda_stream))
+
+        def torch_sort():
+            torch.sort(kd, stable=True)
+
+        ms = _time_sorts(ours, fresh)
+        tms = _time_sorts(torch_sort)
+        ok = torch.equal(v2.cpu().long(),
+                         torch.from_numpy(np.argsort(kd.cpu().numpy().view(np.uint32),
+                                                     kind="stable")))
+        ch = rep.chosen
+        sweep.append({"n": n, "ms": ms, "keys_per_s": n / (ms / 1e3),
+                      "roofline_frac": 68 * n / (ms / 1e3) / 1e9 / peak_gbs,
+                      "digit_bits": ch.radix_digit_bits, "keys_per_thread": ch.radix_items,
+                      "torch_sort_ms": tms, "torch_over_ours": tms / ms,
+                      "stable_sort_checked": bool(ok)})
+        chosen = rep
+    top = sweep[-1]
+    ch = chosen.chosen
+    return {"n": top["n"], "ms": top["ms"], "keys_per_s": top["keys_per_s"],
             "digit_bits": ch.radix_digit_bits, "keys_per_thread": ch.radix_items,
-            "passes": passes, "tuning": rep.as_dict()["radix"]}
+            "passes": -(-32 // ch.radix_digit_bits), "tuning": chosen.as_dict()["radix"],
+            "torch_sort_ms": top["torch_sort_ms"], "sweep": sweep,
+            "timing": "CUDA events around the sort alone, median of 15 after 3 "
+                      "(fresh input copied before each run)"}
 
 
 def full_run(w, params, model, local, frames=None):
@@ -620,7 +665,8 @@ def run_gpu(args) -> None:
     # and the plain solves need many more iterations.
     runs = {}
     if args.full_runs and args.workload == "dam_break_1m":
-        for name in ("dam_break_1m", "dam_break_256k_cfl03"):
+        for name in ("dam_break_1m", "dam_break_1m_cfl03", "dam_break_256k_cfl03",
+                     "dam_break_4m"):
             wr = scene.workload(name)
             r = {}
             for arm in arms:
@@ -635,7 +681,8 @@ def run_gpu(args) -> None:
     splat = splat_benchmark(w, local) if args.full_runs else None
     head = arms["learned"] if "learned" in arms else arms["plain"]
     lib = _abi.load_library()
-    sort = sort_benchmark(lib)
+    peak, peak_kind = load_peaks()
+    sort = sort_benchmark(lib, peak)
 
     kern = head["kern"]
     it_total = head["iters"][0] + head["iters"][1]
@@ -643,7 +690,6 @@ def run_gpu(args) -> None:
              "pressure_update": kern["pressure_update"] * it_total,
              "density_alpha": kern["density_alpha"], "neighbor_search": kern["neighbor_search"]}
     dom = max(("pressure_force", "pressure_update", "density_alpha"), key=lambda k: share[k])
-    peak, peak_kind = load_peaks()
     n = head["n"]
     alg = PASS_BYTES[dom] * n
     achieved = alg / (kern[dom] / 1e3) / 1e9

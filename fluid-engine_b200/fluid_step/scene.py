@@ -142,6 +142,14 @@ def workload(name: str) -> Workload:
         w.params = dam_break_params(w.box_min, w.box_max, use_cfl=True,
                                     solver=_abi.FE_SOLVER_TOLERANCE,
                                     mode=_abi.FE_MODE_FIXED)
+    elif name == "dam_break_1m_cfl03":
+        # the 1M dam break where the solver has work: adaptive CFL (CFL
+        # number 0.3 on h, as the 262k whole run uses), tolerance 0.1 %
+        w = Workload(name, (128, 64, 128), (0.0, 0.0, 0.0), (8.0, 4.0, 8.0), 200)
+        w.params = dam_break_params(w.box_min, w.box_max, use_cfl=True,
+                                    solver=_abi.FE_SOLVER_TOLERANCE,
+                                    mode=_abi.FE_MODE_FIXED)
+        w.params.cfl_lambda = 0.3
     elif name == "dam_break_1m_k4":
         w = Workload(name, (128, 64, 128), (0.0, 0.0, 0.0), (8.0, 4.0, 8.0), 200)
         w.params = dam_break_params(w.box_min, w.box_max)
