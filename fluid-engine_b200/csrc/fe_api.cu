@@ -334,6 +334,10 @@ struct fe_ctx {
     // tuned shapes (fe_autotune / fe_set_tuning)
     RadixConfig radix_cfg = kRadixDefault;
     int mlp_ctas = mlp::kInferDefaultCtasPerSm;
+    // neighbour kernels, per FE_NBR_* group: threads per block, persistent
+    uint32_t nbr_threads[FE_NBR_GROUPS] = {256, 256, 256, 256};
+    uint32_t nbr_persistent[FE_NBR_GROUPS] = {0, 0, 0, 0};
+    int num_sms = 148;
 
     bool learned() const { return params[0].warm_start == FE_WARM_LEARNED && model != nullptr; }
     bool carries() const { return L.carry != nullptr && (learned() || capture); }
@@ -399,6 +403,39 @@ void release(fe_ctx* c) {
 }
 
 dim3 chunk_grid(const fe_ctx* c) { return dim3(c->B.n_chunks); }
+
+// The instantiation of a neighbour kernel for a block size (128, 256, 512)
+// and persistence.
+template <class... KArgs>
+auto pick(void (*k128)(KArgs...), void (*k256)(KArgs...), void (*k512)(KArgs...), uint32_t t)
+    -> void (*)(KArgs...) {
+    return t == 128 ? k128 : t == 512 ? k512 : k256;
+}
+#define NBR_KERNEL_P(name, threads, persist)                                           \
+    ((persist) ? pick(name<128, true>, name<256, true>, name<512, true>, (threads))   \
+               : pick(name<128, false>, name<256, false>, name<512, false>, (threads)))
+#define NBR_KERNEL(name, g) NBR_KERNEL_P(name, c->nbr_threads[g], c->nbr_persistent[g])
+
+// Grid of a neighbour kernel of group g: one block per chunk step (a chunk,
+// two chunks for 512 threads), or, persistent, as many blocks as fit on the
+// GPU at once (each then strides over the chunk table).
+struct NbrGrid {
+    dim3 grid, block;
+};
+NbrGrid nbr_grid(const fe_ctx* c, int g, const void* func) {
+    const uint32_t t = c->nbr_threads[g];
+    const uint32_t per = t >= (uint32_t)kBlock ? t / kBlock : 1u;
+    uint32_t blocks = (c->B.n_chunks + per - 1) / per;
+    if (c->nbr_persistent[g]) {
+        int resident = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, func, (int)t, 0) !=
+                cudaSuccess ||
+            resident < 1)
+            resident = 1;
+        blocks = std::min<uint32_t>(blocks, (uint32_t)resident * (uint32_t)c->num_sms);
+    }
+    return {dim3(blocks > 0 ? blocks : 1), dim3(t)};
+}
 dim3 flat_grid(uint32_t n) { return dim3((n + kBlock - 1) / kBlock); }
 
 // ---------------------------------------------------------------------------
@@ -415,6 +452,66 @@ fe_status rec_check(cudaError_t e, const char* what) {
         fe_status s_ = rec_check((expr), #expr);               \
         if (s_ != FE_OK) return s_;                            \
     } while (0)
+
+// A neighbour kernel of group g with its tuned shape.
+template <class... KArgs, class... Args>
+fe_status rec_nbr(fe_ctx* c, Recorder& R, int g, void (*func)(KArgs...), Args... args) {
+    const NbrGrid G = nbr_grid(c, g, (const void*)func);
+    REC(R.k(func, G.grid, G.block, args...));
+    return FE_OK;
+}
+
+// (128 or 256 threads: the shapes fe_set_tuning accepts for this group)
+fe_status rec_density_alpha(fe_ctx* c, Recorder& R) {
+    const int g = FE_NBR_DENSITY_ALPHA;
+    const uint32_t t = c->nbr_threads[g];
+    return rec_nbr(c, R, g,
+                   c->nbr_persistent[g]
+                       ? pick(k_density_alpha<128, true>, k_density_alpha<256, true>,
+                              k_density_alpha<256, true>, t)
+                       : pick(k_density_alpha<128, false>, k_density_alpha<256, false>,
+                              k_density_alpha<256, false>, t),
+                   c->B);
+}
+
+// Whether a shape may run group g.
+bool nbr_shape_ok(int g, uint32_t threads, uint32_t persistent) {
+    if (persistent > 1) return false;
+    if (g == FE_NBR_PRESSURE_UPDATE) return threads == (uint32_t)kBlock;
+    if (g == FE_NBR_DENSITY_ALPHA) return threads == 128 || threads == 256;
+    return threads == 128 || threads == 256 || threads == 512;
+}
+
+fe_status rec_force(fe_ctx* c, Recorder& R, int which) {
+    return rec_nbr(c, R, FE_NBR_PRESSURE_FORCE,
+                   NBR_KERNEL(k_pressure_force, FE_NBR_PRESSURE_FORCE), c->B, which);
+}
+
+fe_status rec_update(fe_ctx* c, Recorder& R, int which, cudaGraphConditionalHandle h,
+                     int use_handle) {
+    return rec_nbr(c, R, FE_NBR_PRESSURE_UPDATE, k_pressure_update, c->B, which, h, use_handle);
+}
+
+// viscosity and the two source passes (plain or with the learned state)
+fe_status rec_list_pass(fe_ctx* c, Recorder& R, int pass) {
+    const int g = FE_NBR_LIST_PASSES;
+    const int fixed = c->fixed_mode() ? 1 : 0;
+    switch (pass) {
+        case 0: return rec_nbr(c, R, g, NBR_KERNEL(k_viscosity, g), c->B);
+        case 1:
+            if (c->carries())
+                return rec_nbr(c, R, g, NBR_KERNEL(k_density_source_learn, g), c->B, c->L);
+            return rec_nbr(c, R, g, NBR_KERNEL(k_density_source, g), c->B);
+        default:
+            if (c->carries() && fixed)
+                return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source_learn_fixed, g), c->B,
+                               c->L);
+            if (c->carries())
+                return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source_learn, g), c->B, fixed,
+                               c->L);
+            return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source, g), c->B, fixed);
+    }
+}
 
 // NeighborSearch::execute (neighbor_search.rs:176-231).
 fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
@@ -481,9 +578,9 @@ fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
                                 R.stream));
             REC(cudaStreamSynchronize(R.stream));
             if (!cond) break;
-            REC(R.k(k_pressure_force, chunk_grid(c), dim3(kBlock), B, which));
-            REC(R.k(k_pressure_update, chunk_grid(c), dim3(kBlock), B, which,
-                    (cudaGraphConditionalHandle)0, 0));
+            fe_status st;
+            if ((st = rec_force(c, R, which))) return st;
+            if ((st = rec_update(c, R, which, (cudaGraphConditionalHandle)0, 0))) return st;
             if (B.n_scenes > 1)
                 REC(R.k(k_solve_finish, dim3(B.n_scenes), dim3(kBlock), B, which,
                         (cudaGraphConditionalHandle)0, 0));
@@ -508,8 +605,9 @@ fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
     body.stream = R.stream;
     body.graph = cp.conditional.phGraph_out[0];
     body.root = R.root;
-    REC(body.k(k_pressure_force, chunk_grid(c), dim3(kBlock), B, which));
-    REC(body.k(k_pressure_update, chunk_grid(c), dim3(kBlock), B, which, h, 1));
+    fe_status st;
+    if ((st = rec_force(c, body, which))) return st;
+    if ((st = rec_update(c, body, which, h, 1))) return st;
     if (B.n_scenes > 1)  // the per-scene finish, one block per scene
         REC(body.k(k_solve_finish, dim3(B.n_scenes), dim3(kBlock), B, which, h, 1));
     REC(body.k(k_loop_guard, dim3(1), dim3(32), B, which, h));
@@ -551,11 +649,8 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     Bufs B = c->B;
     const int fixed = c->fixed_mode() ? 1 : 0;
     fe_status s;
-    if ((s = rec_simple(c, R, k_viscosity))) return s;
-    if (c->carries())
-        REC(R.k(k_density_source_learn, chunk_grid(c), dim3(kBlock), B, c->L));
-    else if ((s = rec_simple(c, R, k_density_source)))
-        return s;
+    if ((s = rec_list_pass(c, R, 0))) return s;
+    if ((s = rec_list_pass(c, R, 1))) return s;
     if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
         if ((s = rec_trace(c, R, 2 * k))) return s;
@@ -567,13 +662,8 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     else if ((s = rec_simple(c, R, k_pressure_integration)))
         return s;
     if ((s = rec_neighbor_search(c, R))) return s;
-    if ((s = rec_simple(c, R, k_density_alpha))) return s;
-    if (c->carries() && fixed)
-        REC(R.k(k_divergence_source_learn_fixed, chunk_grid(c), dim3(kBlock), B, c->L));
-    else if (c->carries())
-        REC(R.k(k_divergence_source_learn, chunk_grid(c), dim3(kBlock), B, fixed, c->L));
-    else
-        REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), B, fixed));
+    if ((s = rec_density_alpha(c, R))) return s;
+    if ((s = rec_list_pass(c, R, 2))) return s;
     if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
         if ((s = rec_trace(c, R, 2 * k + 1))) return s;
@@ -593,7 +683,7 @@ fe_status rec_frame(fe_ctx* c, Recorder& R, uint32_t n_substeps, bool init) {
     REC(R.k(k_frame_prologue, dim3((c->B.n_scenes + 63) / 64), dim3(64), c->B));
     if (init) {
         if ((s = rec_neighbor_search(c, R))) return s;
-        if ((s = rec_simple(c, R, k_density_alpha))) return s;
+        if ((s = rec_density_alpha(c, R))) return s;
     }
     for (uint32_t k = 0; k < n_substeps; ++k)
         if ((s = rec_substep(c, R, k))) return s;
@@ -937,6 +1027,10 @@ fe_status create_ctx(const fe_params* params, const uint32_t* counts, uint32_t n
         set_error("cudaStreamCreate failed");
         return fail(FE_ERR_CUDA);
     }
+    if (cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device) !=
+            cudaSuccess ||
+        c->num_sms < 1)
+        c->num_sms = 1;
     Bufs& B = c->B;
     std::memset(&B, 0, sizeof B);
     const uint32_t nchunks = (uint32_t)hc.size();
@@ -1322,19 +1416,20 @@ fe_status fe_download_wait(fe_ctx* c, uint64_t ticket) {
     }
 
 FE_STAGE(fe_neighbor_search, return rec_neighbor_search(c, R))
-FE_STAGE(fe_density_alpha, return rec_simple(c, R, k_density_alpha))
-FE_STAGE(fe_viscosity, return rec_simple(c, R, k_viscosity))
-FE_STAGE(fe_density_source, return rec_simple(c, R, k_density_source))
-FE_STAGE(fe_pressure_force, REC(R.k(k_pressure_force, chunk_grid(c), dim3(kBlock), c->B, -1));
-         return FE_OK)
-FE_STAGE(fe_pressure_update,
-         REC(R.k(k_pressure_update, chunk_grid(c), dim3(kBlock), c->B, -1,
-                 (cudaGraphConditionalHandle)0, 0));
-         return FE_OK)
+FE_STAGE(fe_density_alpha, return rec_density_alpha(c, R))
+FE_STAGE(fe_viscosity,
+         return rec_nbr(c, R, FE_NBR_LIST_PASSES,
+                        NBR_KERNEL(k_viscosity, FE_NBR_LIST_PASSES), c->B))
+FE_STAGE(fe_density_source,
+         return rec_nbr(c, R, FE_NBR_LIST_PASSES,
+                        NBR_KERNEL(k_density_source, FE_NBR_LIST_PASSES), c->B))
+FE_STAGE(fe_pressure_force, return rec_force(c, R, -1))
+FE_STAGE(fe_pressure_update, return rec_update(c, R, -1, (cudaGraphConditionalHandle)0, 0))
 FE_STAGE(fe_pressure_integration, return rec_simple(c, R, k_pressure_integration))
 FE_STAGE(fe_divergence_source,
-         REC(R.k(k_divergence_source, chunk_grid(c), dim3(kBlock), c->B, c->fixed_mode() ? 1 : 0));
-         return FE_OK)
+         return rec_nbr(c, R, FE_NBR_LIST_PASSES,
+                        NBR_KERNEL(k_divergence_source, FE_NBR_LIST_PASSES),
+                        c->B, c->fixed_mode() ? 1 : 0))
 FE_STAGE(fe_divergence_integration,
          REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), c->B,
                  c->fixed_mode() ? 1 : 0));
@@ -1846,6 +1941,109 @@ void fill_radix_report(fe_tune_report* r, const float* ms) {
 
 }  // namespace
 
+// Neighbour-kernel shapes: every candidate of every group is timed on the
+// context's current state (one untimed launch, then the median of 7 CUDA-
+// event timed launches, eager, on the context stream).  Some of the timed
+// passes write state (the sources reset the pressures, the update advances
+// them), so the state is exported to host memory first and imported again
+// at the end: the next frame starts from exactly the state it had.
+constexpr uint32_t kNbrCandThreads[] = {128, 256, 512, 128, 256, 512};
+constexpr uint32_t kNbrCandPersistent[] = {0, 0, 0, 1, 1, 1};
+constexpr int kNbrCands = 6;
+
+fe_status time_nbr_group(fe_ctx* c, int g, float* ms_out) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    FE_CUDA(cudaEventCreate(&a));
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        set_error("cudaEventCreate failed");
+        return FE_ERR_CUDA;
+    }
+    Recorder R = eager(c);
+    auto launch = [&]() -> fe_status {
+        switch (g) {
+            case FE_NBR_DENSITY_ALPHA: return rec_density_alpha(c, R);
+            case FE_NBR_LIST_PASSES: {
+                fe_status st;
+                for (int pass = 0; pass < 3; ++pass)
+                    if ((st = rec_list_pass(c, R, pass)) != FE_OK) return st;
+                return FE_OK;
+            }
+            case FE_NBR_PRESSURE_FORCE: return rec_force(c, R, -1);
+            default: return rec_update(c, R, -1, (cudaGraphConditionalHandle)0, 0);
+        }
+    };
+    std::vector<float> t;
+    fe_status st = FE_OK;
+    for (int rep = 0; rep < 8 && st == FE_OK; ++rep) {
+        cudaEventRecord(a, c->stream);
+        st = launch();
+        cudaEventRecord(b, c->stream);
+        if (st == FE_OK && cudaEventSynchronize(b) == cudaSuccess) {
+            float v = 0.0f;
+            cudaEventElapsedTime(&v, a, b);
+            if (rep > 0) t.push_back(v);
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (st != FE_OK) return st;
+    if (t.empty()) {
+        set_error("neighbour tuning: timing failed");
+        return FE_ERR_CUDA;
+    }
+    std::sort(t.begin(), t.end());
+    *ms_out = t[t.size() / 2];
+    return FE_OK;
+}
+
+fe_status tune_neighbour_kernels(fe_ctx* c, fe_tune_report* r) {
+    size_t bytes = 0;
+    fe_status st = fe_state_size(c, &bytes);
+    if (st != FE_OK) return st;
+    std::vector<unsigned char> snap(bytes);
+    if ((st = fe_state_export(c, snap.data(), bytes)) != FE_OK) return st;
+    r->nbr_candidates = kNbrCands;
+    for (int k = 0; k < kNbrCands; ++k) {
+        r->nbr_threads[k] = kNbrCandThreads[k];
+        r->nbr_persistent[k] = kNbrCandPersistent[k];
+    }
+    uint32_t best_t[FE_NBR_GROUPS], best_p[FE_NBR_GROUPS];
+    for (int g = 0; g < FE_NBR_GROUPS; ++g) {
+        const uint32_t keep_t = c->nbr_threads[g], keep_p = c->nbr_persistent[g];
+        float best = -1.0f;
+        best_t[g] = keep_t;
+        best_p[g] = keep_p;
+        for (int k = 0; k < kNbrCands; ++k) {
+            r->nbr_ms[g][k] = -1.0f;
+            if (!nbr_shape_ok(g, kNbrCandThreads[k], kNbrCandPersistent[k])) continue;
+            c->nbr_threads[g] = kNbrCandThreads[k];
+            c->nbr_persistent[g] = kNbrCandPersistent[k];
+            float ms = 0.0f;
+            if ((st = time_nbr_group(c, g, &ms)) != FE_OK) break;
+            r->nbr_ms[g][k] = ms;
+            if (best < 0.0f || ms < best) {
+                best = ms;
+                best_t[g] = kNbrCandThreads[k];
+                best_p[g] = kNbrCandPersistent[k];
+            }
+        }
+        c->nbr_threads[g] = keep_t;
+        c->nbr_persistent[g] = keep_p;
+        if (st != FE_OK) break;
+    }
+    if (st == FE_OK)
+        for (int g = 0; g < FE_NBR_GROUPS; ++g) {
+            c->nbr_threads[g] = best_t[g];
+            c->nbr_persistent[g] = best_p[g];
+        }
+    // the state as it was (the import rebuilds the neighbour list with the
+    // chosen density_alpha shape: the same list)
+    fe_status st2 = fe_state_import(c, snap.data(), bytes);
+    drop_graphs(c);
+    return st != FE_OK ? st : st2;
+}
+
 fe_status fe_autotune(fe_ctx* c, fe_tune_report* report) {
     if (!c) {
         set_error("context is NULL");
@@ -1900,9 +2098,19 @@ fe_status fe_autotune(fe_ctx* c, fe_tune_report* report) {
     drop_graphs(c);  // recorded frames hold the previous shapes
     c->radix_cfg = best;
     c->mlp_ctas = ctas;
+    // (not while training data is captured: the learned source passes would
+    // record extra samples while they are timed)
+    if (c->initialized && !c->capture) {
+        fe_status st = tune_neighbour_kernels(c, &r);
+        if (st != FE_OK) return st;
+    }
     r.chosen.radix_digit_bits = best.digit_bits;
     r.chosen.radix_items = best.items;
     r.chosen.mlp_ctas_per_sm = (uint32_t)ctas;
+    for (int g = 0; g < FE_NBR_GROUPS; ++g) {
+        r.chosen.nbr_threads[g] = c->nbr_threads[g];
+        r.chosen.nbr_persistent[g] = c->nbr_persistent[g];
+    }
     if (report) *report = r;
     return FE_OK;
 }
@@ -1916,6 +2124,10 @@ fe_status fe_get_tuning(const fe_ctx* c, fe_tuning* out) {
     out->radix_digit_bits = c->radix_cfg.digit_bits;
     out->radix_items = c->radix_cfg.items;
     out->mlp_ctas_per_sm = (uint32_t)c->mlp_ctas;
+    for (int g = 0; g < FE_NBR_GROUPS; ++g) {
+        out->nbr_threads[g] = c->nbr_threads[g];
+        out->nbr_persistent[g] = c->nbr_persistent[g];
+    }
     return FE_OK;
 }
 
@@ -1934,10 +2146,23 @@ fe_status fe_set_tuning(fe_ctx* c, const fe_tuning* t) {
         set_error("mlp_ctas_per_sm %u outside 1..%d", t->mlp_ctas_per_sm, mlp::kInferMaxCtasPerSm);
         return FE_ERR_INVALID_ARGUMENT;
     }
+    uint32_t nt[FE_NBR_GROUPS];
+    for (int g = 0; g < FE_NBR_GROUPS; ++g) {
+        nt[g] = t->nbr_threads[g] ? t->nbr_threads[g] : (uint32_t)kBlock;
+        if (!nbr_shape_ok(g, nt[g], t->nbr_persistent[g])) {
+            set_error("neighbour group %d: %u threads per block, persistent %u is not a "
+                      "candidate", g, t->nbr_threads[g], t->nbr_persistent[g]);
+            return FE_ERR_INVALID_ARGUMENT;
+        }
+    }
     FE_CUDA(cudaSetDevice(c->device));
     drop_graphs(c);
     c->radix_cfg = cfg;
     c->mlp_ctas = (int)t->mlp_ctas_per_sm;
+    for (int g = 0; g < FE_NBR_GROUPS; ++g) {
+        c->nbr_threads[g] = nt[g];
+        c->nbr_persistent[g] = t->nbr_persistent[g];
+    }
     return FE_OK;
 }
 
@@ -2229,7 +2454,7 @@ FE_API fe_status fe_state_import(fe_ctx* c, const void* src, size_t bytes) {
     // p / rho^2.  The global flags are restored after it.
     if (hd.initialized) {
         Recorder R = eager(c);
-        if ((s = rec_simple(c, R, k_density_alpha)) != FE_OK) return s;
+        if ((s = rec_density_alpha(c, R)) != FE_OK) return s;
     }
     FE_CUDA(cudaMemcpyAsync(c->B.G, global, sizeof(GlobalState), cudaMemcpyHostToDevice,
                             c->stream));

@@ -296,15 +296,17 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
     }
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
-    __shared__ DensityScratch scratch[kBlock / 32];
-    uint32_t i, s, c;
-    const bool live = chunk_of(B, i, s, c);
+// Blocks per SM the launch bounds ask for: 1024 resident threads per SM
+// (at most 64 registers per thread), for every block size.
+template <int kThreads>
+constexpr int kMinBlocks = 1024 / kThreads;
+
+__device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScratch& S,
+                                                       uint32_t i, uint32_t s, bool live) {
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
     const float kn = kernel_norm(h);
     const int lane = lane_id();
-    DensityScratch& S = scratch[threadIdx.x >> 5];
     const float4 p4 = live ? __ldg(posb(B, i)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const f3 pi = xyz(p4);
     const int cx = cell_coord(pi.x, h), cy = cell_coord(pi.y, h), cz = cell_coord(pi.z, h);
@@ -374,12 +376,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_density_alpha(Bufs B) {
     if (a.cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
 }
 
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_density_alpha(Bufs B) {
+    __shared__ DensityScratch scratch[kThreads / 32];
+    DensityScratch& S = scratch[threadIdx.x >> 5];
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        density_alpha_particle(B, S, i, s, live);
+    });
+}
+
 // ---------------------------------------------------------------------------
 // viscosity.comp:17-66: velocity_b in, velocity_a out.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
-    uint32_t i, s, c;
-    if (!chunk_of(B, i, s, c)) return;
+__device__ __forceinline__ void viscosity_particle(const Bufs& B, uint32_t i, uint32_t s) {
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
     const f3 pi = xyz(__ldg(posb(B, i)));
@@ -404,6 +413,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_viscosity(Bufs B) {
             make_float4(vf.x, vf.y, vf.z, B.rho[i]));
 }
 
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_viscosity(Bufs B) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live) viscosity_particle(B, i, s);
+    });
+}
+
 // ---------------------------------------------------------------------------
 // density_source_term.comp:16-74 (velocities = velocity_a).  The kLearn
 // variant also emits the warm-start features (same arithmetic for s and p).
@@ -414,9 +430,8 @@ struct VelRho {
 };
 
 template <bool kLearn>
-__device__ __forceinline__ void density_source_body(const Bufs& B, const LearnArgs& L) {
-    uint32_t i, s, c;
-    if (!chunk_of(B, i, s, c)) return;
+__device__ __forceinline__ void density_source_body(const Bufs& B, const LearnArgs& L,
+                                                    uint32_t i, uint32_t s) {
     const DevParams& P = B.P[s];
     const float m = P.mass, dt = P.dt;
     const f3 pi = xyz(__ldg(posb(B, i)));
@@ -439,11 +454,18 @@ __device__ __forceinline__ void density_source_body(const Bufs& B, const LearnAr
     if (kLearn) emit_features(B, L, P, i, s, 0, div, vi, mo);
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_density_source(Bufs B) {
-    density_source_body<false>(B, LearnArgs{});
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_density_source(Bufs B) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live) density_source_body<false>(B, LearnArgs{}, i, s);
+    });
 }
-__global__ void __launch_bounds__(kBlock, 3) k_density_source_learn(Bufs B, LearnArgs L) {
-    density_source_body<true>(B, L);
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, (3 * kMinBlocks<kThreads>) / 4)
+    k_density_source_learn(Bufs B, LearnArgs L) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live) density_source_body<true>(B, L, i, s);
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -452,9 +474,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_density_source_learn(Bufs B, Lear
 // ---------------------------------------------------------------------------
 template <bool kLearn>
 __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
-                                                       const LearnArgs& L) {
-    uint32_t i, s, c;
-    if (!chunk_of(B, i, s, c)) return;
+                                                       const LearnArgs& L, uint32_t i,
+                                                       uint32_t s) {
     const DevParams& P = B.P[s];
     const float m = P.mass;
     const f3 pi = xyz(__ldg(posb(B, i)));
@@ -483,27 +504,35 @@ __device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
     if (kLearn) emit_features(B, L, P, i, s, 1, div, vi, mo);
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_divergence_source(Bufs B, int fixed) {
-    divergence_source_body<false>(B, fixed, LearnArgs{});
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_divergence_source(Bufs B,
+                                                                                      int fixed) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live) divergence_source_body<false>(B, fixed, LearnArgs{}, i, s);
+    });
 }
 // FIXED mode with the learned state: the mode is a constant, so only the
-// record path is compiled (fewer registers, four blocks per SM).
-__global__ void __launch_bounds__(kBlock, 4) k_divergence_source_learn_fixed(Bufs B, LearnArgs L) {
-    divergence_source_body<true>(B, 1, L);
+// record path is compiled (fewer registers, four blocks of 256 per SM).
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
+    k_divergence_source_learn_fixed(Bufs B, LearnArgs L) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live) divergence_source_body<true>(B, 1, L, i, s);
+    });
 }
-__global__ void __launch_bounds__(kBlock, 3) k_divergence_source_learn(Bufs B, int fixed,
-                                                                        LearnArgs L) {
-    divergence_source_body<true>(B, fixed, L);
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, (3 * kMinBlocks<kThreads>) / 4)
+    k_divergence_source_learn(Bufs B, int fixed, LearnArgs L) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live) divergence_source_body<true>(B, fixed, L, i, s);
+    });
 }
 
 // ---------------------------------------------------------------------------
 // pressure_force.comp:15-78.  pr[j] = p_j / rho_j^2 (NaN when rho_j <= 1e-6)
 // is maintained by every pass that writes p or rho.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which) {
-    uint32_t i, s, c;
-    if (!chunk_of(B, i, s, c)) return;
-    if (which >= 0 && B.S[s].solve[which].done) return;
+__device__ __forceinline__ void pressure_force_particle(const Bufs& B, uint32_t i, uint32_t s) {
     const DevParams& P = B.P[s];
     const float m = P.mass;
     const float4 p4 = __ldg(posb(B, i));
@@ -525,6 +554,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_pressure_force(Bufs B, int which)
     // the whole record: this particle's position for pressure_update's
     // gathers and its acceleration
     st_record(B, i, p4, make_float4(-acc.x, -acc.y, -acc.z, 0.0f));
+}
+
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_pressure_force(Bufs B,
+                                                                                   int which) {
+    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+        if (live && !(which >= 0 && B.S[s].solve[which].done)) pressure_force_particle(B, i, s);
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -623,58 +660,63 @@ __global__ void __launch_bounds__(kBlock) k_solve_finish(Bufs B, int which,
     }
 }
 
+// One block per chunk, or a persistent grid whose blocks stride over the
+// chunks (the per-chunk partials, and so the sums, are the same).
 __global__ void __launch_bounds__(kBlock) k_pressure_update(Bufs B, int which,
                                                             cudaGraphConditionalHandle handle,
                                                             int use_handle) {
     __shared__ double smem[8];
-    uint32_t i, s, c;
-    bool valid = chunk_of(B, i, s, c);
-    const DevParams& P = B.P[s];
     const bool control = which >= 0;
-    const bool skip = control && B.S[s].solve[which].done;
-    double e_sum_in = 0.0;
-    if (valid && !skip) {
-        const float m = P.mass, dt = P.dt, omega = P.omega;
-        const f3 pi = xyz(__ldg(posb(B, i)));
-        const f3 ai = xyz(*accp(B, i));
-        float sum_ap = 0.0f;
-        for_each_neighbor_record(B, P, i, pi, [&](f3 rv, float g, float4 aj) {
-            f3 grad = scale(g, rv);
-            f3 ad = sub(ai, xyz(aj));
-            sum_ap += m * dot(ad, grad);
-        });
-        const float alpha_i = B.alpha[i], rho_i = B.rho[i], s_i = B.src[i], p_i = B.prs[i];
-        float ap_i = dt * sum_ap;
-        float error = s_i - ap_i;
-        float p_new = p_i;
-        float e = 0.0f;
-        if (alpha_i > kEpsR && rho_i > kEpsR) {
-            float a_ii = -(dt / (rho_i * rho_i)) * alpha_i;
-            if (fabsf(a_ii) > 1e-20f) {
-                float corr = (omega * error) / a_ii;
-                float np = p_i + corr;
-                p_new = np > 0.0f ? np : 0.0f;
-                B.prs[i] = p_new;
-                e = np > 0.0f ? fabsf(error) : (p_i * fabsf(a_ii)) / omega;
+    for (uint32_t c = blockIdx.x; c < B.n_chunks; c += gridDim.x) {
+        const uint4 cc = B.chunks[c];
+        const uint32_t i = cc.x + threadIdx.x, s = cc.z;
+        const bool valid = threadIdx.x < cc.y;
+        const DevParams& P = B.P[s];
+        const bool skip = control && B.S[s].solve[which].done;
+        double e_sum_in = 0.0;
+        if (valid && !skip) {
+            const float m = P.mass, dt = P.dt, omega = P.omega;
+            const f3 pi = xyz(__ldg(posb(B, i)));
+            const f3 ai = xyz(*accp(B, i));
+            float sum_ap = 0.0f;
+            for_each_neighbor_record(B, P, i, pi, [&](f3 rv, float g, float4 aj) {
+                f3 grad = scale(g, rv);
+                f3 ad = sub(ai, xyz(aj));
+                sum_ap += m * dot(ad, grad);
+            });
+            const float alpha_i = B.alpha[i], rho_i = B.rho[i], s_i = B.src[i], p_i = B.prs[i];
+            float ap_i = dt * sum_ap;
+            float error = s_i - ap_i;
+            float p_new = p_i;
+            float e = 0.0f;
+            if (alpha_i > kEpsR && rho_i > kEpsR) {
+                float a_ii = -(dt / (rho_i * rho_i)) * alpha_i;
+                if (fabsf(a_ii) > 1e-20f) {
+                    float corr = (omega * error) / a_ii;
+                    float np = p_i + corr;
+                    p_new = np > 0.0f ? np : 0.0f;
+                    B.prs[i] = p_new;
+                    e = np > 0.0f ? fabsf(error) : (p_i * fabsf(a_ii)) / omega;
+                }
+            }
+            posb(B, i)->w = pressure_over_rho2(p_new, rho_i);
+            if (control && P.solver == 1u) {
+                if (which == 0) e = dt * e;
+                e_sum_in = e > 0.0f ? (double)e : 0.0;  // NaN -> 0
             }
         }
-        posb(B, i)->w = pressure_over_rho2(p_new, rho_i);
-        if (control && P.solver == 1u) {
-            if (which == 0) e = dt * e;
-            e_sum_in = e > 0.0f ? (double)e : 0.0;  // NaN -> 0
+        // Per-chunk partial of the fixed-order sum and the chunk's largest
+        // error (uniform branch per block).
+        if (control && !skip && P.solver == 1u) {
+            double part = block_tree256(e_sum_in, smem);
+            double mx = block_max256(e_sum_in, smem);
+            if (threadIdx.x == 0) {
+                B.partials[c] = part;
+                B.partials[B.n_chunks + c] = mx;
+            }
         }
     }
     if (!control) return;
-    // Per-chunk partial of the fixed-order sum and the chunk's largest error
-    // (uniform branch per block).
-    if (!skip && P.solver == 1u) {
-        double part = block_tree256(e_sum_in, smem);
-        double mx = block_max256(e_sum_in, smem);
-        if (threadIdx.x == 0) {
-            B.partials[c] = part;
-            B.partials[B.n_chunks + c] = mx;
-        }
-    }
     // One scene: its last block finishes the iteration.  Several scenes:
     // k_solve_finish does, one block per scene.
     if (B.n_scenes == 1 && last_block_done(&B.G->tickets[kTicketSolve], gridDim.x)) {
@@ -965,5 +1007,27 @@ __global__ void k_count_substep(Bufs B) {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < B.n_scenes) B.S[s].substeps += 1;
 }
+
+// The block sizes the autotuner chooses from.
+// (density_alpha: 128 and 256 only; its per-warp scratch would exceed the
+// 48 KB of static shared memory of a block at 512 threads)
+#define FE_NBR_INSTANTIATE(T, P)                                                      \
+    template __global__ void k_viscosity<T, P>(Bufs);                                 \
+    template __global__ void k_density_source<T, P>(Bufs);                            \
+    template __global__ void k_density_source_learn<T, P>(Bufs, LearnArgs);           \
+    template __global__ void k_divergence_source<T, P>(Bufs, int);                    \
+    template __global__ void k_divergence_source_learn<T, P>(Bufs, int, LearnArgs);   \
+    template __global__ void k_divergence_source_learn_fixed<T, P>(Bufs, LearnArgs);  \
+    template __global__ void k_pressure_force<T, P>(Bufs, int);
+FE_NBR_INSTANTIATE(128, false)
+FE_NBR_INSTANTIATE(256, false)
+FE_NBR_INSTANTIATE(512, false)
+FE_NBR_INSTANTIATE(128, true)
+FE_NBR_INSTANTIATE(256, true)
+FE_NBR_INSTANTIATE(512, true)
+template __global__ void k_density_alpha<128, false>(Bufs);
+template __global__ void k_density_alpha<256, false>(Bufs);
+template __global__ void k_density_alpha<128, true>(Bufs);
+template __global__ void k_density_alpha<256, true>(Bufs);
 
 }  // namespace fe

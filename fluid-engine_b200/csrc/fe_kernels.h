@@ -9,6 +9,10 @@
 
 namespace fe {
 
+// The neighbour kernels are templates over their block size (128, 256 or
+// 512 threads) and persistence (a grid of resident blocks striding over the
+// chunks, or one block per chunk step; see for_each_particle in
+// fe_neighbors.cuh), instantiated for those shapes in fe_kernels.cu.
 __global__ void k_fill_u32(uint32_t* p, uint32_t v, size_t count);
 __global__ void k_fill_cells(uint2* p, size_t count);
 __global__ void k_hash(Bufs B);
@@ -18,14 +22,19 @@ __global__ void k_reorder_carry(Bufs B, int carry_pressure, LearnArgs L);
 __global__ void k_take_pressure(Bufs B);
 __global__ void k_take_pressure_carry(Bufs B, LearnArgs L);
 __global__ void k_refresh_pr(Bufs B);
+template <int kThreads, bool kPersist>
 __global__ void k_density_alpha(Bufs B);
+template <int kThreads, bool kPersist>
 __global__ void k_viscosity(Bufs B);
 // Per-scene finishes of a multi-scene context, one block per scene.
 __global__ void k_solve_finish(Bufs B, int which, cudaGraphConditionalHandle handle,
                                int use_handle);
 __global__ void k_stats_finish(Bufs B, uint4* upart);
+template <int kThreads, bool kPersist>
 __global__ void k_density_source(Bufs B);
+template <int kThreads, bool kPersist>
 __global__ void k_divergence_source(Bufs B, int fixed);
+template <int kThreads, bool kPersist>
 __global__ void k_pressure_force(Bufs B, int which);
 __global__ void k_pressure_update(Bufs B, int which, cudaGraphConditionalHandle handle,
                                   int use_handle);
@@ -40,8 +49,11 @@ __global__ void k_divergence_integration_learn(Bufs B, int fixed, LearnArgs L);
 __global__ void k_stats(Bufs B, int fixed, uint4* upart);
 __global__ void k_frame_prologue(Bufs B);
 __global__ void k_count_substep(Bufs B);
+template <int kThreads, bool kPersist>
 __global__ void k_density_source_learn(Bufs B, LearnArgs L);
+template <int kThreads, bool kPersist>
 __global__ void k_divergence_source_learn(Bufs B, int fixed, LearnArgs L);
+template <int kThreads, bool kPersist>
 __global__ void k_divergence_source_learn_fixed(Bufs B, LearnArgs L);
 __global__ void k_warm_apply(Bufs B, LearnArgs L, int which);
 __global__ void k_carry_take(Bufs B, LearnArgs L);

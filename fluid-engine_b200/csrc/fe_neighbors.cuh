@@ -16,6 +16,48 @@ __device__ __forceinline__ bool chunk_of(const Bufs& B, uint32_t& i, uint32_t& s
     return threadIdx.x < c.y;
 }
 
+// Block-size-agnostic particle loop of the neighbour kernels over the chunk
+// table (the scene-offset table: every chunk is <= 256 consecutive particles
+// of one scene).  A block of kThreads threads takes kThreads / 256 chunks at a
+// time (512), or one chunk in 256 / kThreads passes (128); a grid smaller
+// than the chunk count makes the kernel persistent: each block strides over
+// the chunks until all are done.  Every warp covers 32 consecutive particles
+// of one chunk, so warp-level cooperation and per-particle results are the
+// same for every shape.  f(i, scene, live) is called by every thread of a
+// warp together (live: i is a particle of the chunk).
+template <int kThreads>
+struct ParticleLoop {
+    static_assert(kThreads == 128 || kThreads == 256 || kThreads == 512, "block size");
+    static constexpr uint32_t kChunksPerStep = kThreads >= kBlock ? kThreads / kBlock : 1;
+    static constexpr uint32_t kPasses = kThreads >= kBlock ? 1 : kBlock / kThreads;
+};
+
+// kPersist = false: the grid has one block per chunk step and the loop
+// below runs once (compiled without the loop state).
+template <int kThreads, bool kPersist, class F>
+__device__ __forceinline__ void for_each_particle(const Bufs& B, F&& f) {
+    using L = ParticleLoop<kThreads>;
+    const uint32_t sub = kThreads >= kBlock ? threadIdx.x / kBlock : 0u;
+    const uint32_t t = kThreads >= kBlock ? threadIdx.x % kBlock : threadIdx.x;
+    auto step = [&](uint32_t c0) {
+        const uint32_t c = c0 + sub;
+        if (c >= B.n_chunks) return;   // whole warps: sub is uniform per 256 threads
+        const uint4 cc = B.chunks[c];
+#pragma unroll 1
+        for (uint32_t k = 0; k < L::kPasses; ++k) {
+            const uint32_t off = k * kThreads + t;
+            f(cc.x + off, cc.z, off < cc.y);
+        }
+    };
+    if constexpr (kPersist) {
+        for (uint32_t c0 = blockIdx.x * L::kChunksPerStep; c0 < B.n_chunks;
+             c0 += gridDim.x * L::kChunksPerStep)
+            step(c0);
+    } else {
+        step(blockIdx.x * L::kChunksPerStep);
+    }
+}
+
 // The bucket walk of the shaders (e.g. density_and_alpha.comp:31-63) over the
 // {start, end} table.  f(j, r_vec, r2) is called for each candidate with
 // r2 <= h*h, in walk order.

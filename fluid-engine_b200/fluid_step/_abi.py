@@ -12,7 +12,7 @@ import os
 from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
                     c_int32, c_size_t, c_uint32, c_uint64, c_void_p)
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 FE_STATE_VERSION = 3
 
 # fe_status
@@ -156,10 +156,34 @@ class FeCamera(Structure):
                 ("width", c_uint32), ("height", c_uint32), ("reserved", c_uint32 * 3)]
 
 
+FE_NBR_DENSITY_ALPHA = 0
+FE_NBR_LIST_PASSES = 1
+FE_NBR_PRESSURE_FORCE = 2
+FE_NBR_PRESSURE_UPDATE = 3
+FE_NBR_GROUPS = 4
+NBR_GROUP_NAMES = ("density_alpha", "list_passes", "pressure_force", "pressure_update")
+
+
 class FeTuning(Structure):
     """fe_tuning: the tunable shapes (none changes a result)."""
     _fields_ = [("radix_digit_bits", c_uint32), ("radix_items", c_uint32),
-                ("mlp_ctas_per_sm", c_uint32), ("reserved", c_uint32)]
+                ("mlp_ctas_per_sm", c_uint32), ("reserved", c_uint32),
+                ("nbr_threads", c_uint32 * FE_NBR_GROUPS),
+                ("nbr_persistent", c_uint32 * FE_NBR_GROUPS)]
+
+    def as_dict(self) -> dict:
+        return {"radix_digit_bits": self.radix_digit_bits, "radix_items": self.radix_items,
+                "mlp_ctas_per_sm": self.mlp_ctas_per_sm,
+                "nbr_threads": list(self.nbr_threads),
+                "nbr_persistent": list(self.nbr_persistent)}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "FeTuning":
+        t = cls(int(d["radix_digit_bits"]), int(d["radix_items"]), int(d["mlp_ctas_per_sm"]), 0)
+        for g in range(FE_NBR_GROUPS):
+            t.nbr_threads[g] = int(d.get("nbr_threads", [256] * FE_NBR_GROUPS)[g])
+            t.nbr_persistent[g] = int(d.get("nbr_persistent", [0] * FE_NBR_GROUPS)[g])
+        return t
 
 
 FE_TUNE_MAX_CANDIDATES = 8
@@ -174,6 +198,10 @@ class FeTuneReport(Structure):
                 ("mlp_candidates", c_uint32),
                 ("mlp_ctas_per_sm", c_uint32 * FE_TUNE_MAX_CANDIDATES),
                 ("mlp_ms", c_float * FE_TUNE_MAX_CANDIDATES),
+                ("nbr_candidates", c_uint32),
+                ("nbr_threads", c_uint32 * FE_TUNE_MAX_CANDIDATES),
+                ("nbr_persistent", c_uint32 * FE_TUNE_MAX_CANDIDATES),
+                ("nbr_ms", (c_float * FE_TUNE_MAX_CANDIDATES) * FE_NBR_GROUPS),
                 ("chosen", FeTuning)]
 
     def as_dict(self) -> dict:
@@ -181,9 +209,12 @@ class FeTuneReport(Structure):
                         "ms": self.radix_ms[k]} for k in range(self.radix_candidates)],
              "mlp": [{"ctas_per_sm": self.mlp_ctas_per_sm[k], "ms": self.mlp_ms[k]}
                      for k in range(self.mlp_candidates)],
-             "chosen": {"radix_digit_bits": self.chosen.radix_digit_bits,
-                        "radix_items": self.chosen.radix_items,
-                        "mlp_ctas_per_sm": self.chosen.mlp_ctas_per_sm}}
+             "neighbour": {NBR_GROUP_NAMES[g]: [
+                 {"threads": self.nbr_threads[k], "persistent": self.nbr_persistent[k],
+                  "ms": self.nbr_ms[g][k]}
+                 for k in range(self.nbr_candidates) if self.nbr_ms[g][k] >= 0]
+                 for g in range(FE_NBR_GROUPS)},
+             "chosen": self.chosen.as_dict()}
         return r
 
 

@@ -1,8 +1,9 @@
 """Autotuning with a persistent cache of earlier measurements.
 
 fe_autotune times every candidate shape of the tunable kernels (radix digit
-width and keys per thread, the inference grid) on the context's own device
-and data and applies the fastest.  `tune` keeps those choices in a JSON file
+width and keys per thread, the inference grid, threads per block and
+persistence of the neighbour kernels) on the context's own device and data
+and applies the fastest.  `tune` keeps those choices in a JSON file
 keyed by GPU model, SM count, problem size class and key width, so that a
 later context of the same class on the same kind of GPU applies the cached
 choice without timing anything.
@@ -60,9 +61,7 @@ def tune(data, cache_path: str | None = None, *, learned: bool = False,
     cache = load_cache(cache_path)
     if key in cache:
         c = cache[key]
-        t = _abi.FeTuning(int(c["radix_digit_bits"]), int(c["radix_items"]),
-                          int(c["mlp_ctas_per_sm"]), 0)
-        data.set_tuning(t)
+        data.set_tuning(_abi.FeTuning.from_dict(c))
         return {"source": "cache", "key": key, "tuning": dict(c)}
     report = data.autotune()
     rd = report.as_dict()

@@ -38,7 +38,7 @@ extern "C" {
 #define FE_API
 #endif
 
-#define FE_ABI_VERSION 1u
+#define FE_ABI_VERSION 2u
 
 /* ------------------------------------------------------------------------- */
 /* Status codes                                                              */
@@ -465,16 +465,34 @@ FE_API fe_status fe_sort_flags(uint32_t* flags_out, void* stream);
 /* Autotuning (no reference counterpart: the reference fixes its workgroup   */
 /* sizes and 8-bit digits in the shaders)                                     */
 /* ------------------------------------------------------------------------- */
+/* Groups of neighbour-loop kernels that share a launch shape. */
+#define FE_NBR_DENSITY_ALPHA 0   /* density_alpha: bucket walk, neighbour list */
+#define FE_NBR_LIST_PASSES 1     /* viscosity and the density/divergence sources */
+#define FE_NBR_PRESSURE_FORCE 2  /* pressure_force (Jacobi A p, first half) */
+#define FE_NBR_PRESSURE_UPDATE 3 /* pressure_update (second half, residual sums) */
+#define FE_NBR_GROUPS 4
+
 /* Tunable shapes; none of them changes a result.
  *   radix_digit_bits, radix_items: onesweep digit width (8 or 10) and keys
  *     per thread (4, 8, 16; the pairs (8,4) (8,8) (8,16) (10,8) (10,16)).
  *   mlp_ctas_per_sm: blocks per SM of the learned warm start's inference
- *     grid (1..6). */
+ *     grid (1..6).
+ *   nbr_threads[g]: threads per block of neighbour group g, 128, 256 or 512
+ *     (a block covers half a 256-particle chunk per pass, one chunk, or two
+ *     chunks at a time; particles per thread = 256 / threads per chunk);
+ *     FE_NBR_DENSITY_ALPHA 128 or 256 (its per-warp shared scratch),
+ *     FE_NBR_PRESSURE_UPDATE 256 only, its FP64 sums being per chunk.  0
+ *     means 256.
+ *   nbr_persistent[g]: 1 = persistent grid (as many blocks as fit on the
+ *     GPU at once, each striding over the chunk table of all scenes); 0 =
+ *     one block per chunk (or chunk pair). */
 typedef struct fe_tuning {
     uint32_t radix_digit_bits;
     uint32_t radix_items;
     uint32_t mlp_ctas_per_sm;
     uint32_t reserved;
+    uint32_t nbr_threads[FE_NBR_GROUPS];
+    uint32_t nbr_persistent[FE_NBR_GROUPS];
 } fe_tuning;
 
 #define FE_TUNE_MAX_CANDIDATES 8
@@ -488,14 +506,23 @@ typedef struct fe_tune_report {
     uint32_t mlp_candidates;                 /* 0: no model attached */
     uint32_t mlp_ctas_per_sm[FE_TUNE_MAX_CANDIDATES];
     float mlp_ms[FE_TUNE_MAX_CANDIDATES];
+    /* neighbour kernels (0 candidates before the first neighbour search):
+     * the shared candidate list, and per group the median time of each
+     * candidate, negative where it is not a candidate of that group */
+    uint32_t nbr_candidates;
+    uint32_t nbr_threads[FE_TUNE_MAX_CANDIDATES];
+    uint32_t nbr_persistent[FE_TUNE_MAX_CANDIDATES];
+    float nbr_ms[FE_NBR_GROUPS][FE_TUNE_MAX_CANDIDATES];
     fe_tuning chosen;
 } fe_tune_report;
 
 /* Times the candidate shapes on this context's device and data (the sort on
  * the hashes of the current positions; the network on the current feature
- * rows when a model is attached), applies the fastest and drops the
- * recorded frame graphs.  Synchronises the context; allocates temporary
- * device memory.  `report` may be NULL. */
+ * rows when a model is attached; each neighbour group's kernels on the
+ * current state, which is saved to host memory first and restored bit for
+ * bit afterwards), applies the fastest and drops the recorded frame graphs.
+ * Synchronises the context; allocates temporary device memory.  `report`
+ * may be NULL. */
 FE_API fe_status fe_autotune(fe_ctx* ctx, fe_tune_report* report);
 /* The context's current shapes, and setting them (e.g. from a cache of
  * earlier tuning runs).  FE_ERR_INVALID_ARGUMENT for a shape outside the

@@ -14,7 +14,8 @@ class FakeData:
         self.measured = 0
 
     def set_tuning(self, t):
-        self.applied = (t.radix_digit_bits, t.radix_items, t.mlp_ctas_per_sm)
+        self.applied = (t.radix_digit_bits, t.radix_items, t.mlp_ctas_per_sm,
+                        list(t.nbr_threads), list(t.nbr_persistent))
 
     def autotune(self):
         self.measured += 1
@@ -23,6 +24,8 @@ class FakeData:
         r.radix_digit_bits[0], r.radix_items[0], r.radix_ms[0] = 8, 16, 0.2
         r.radix_digit_bits[1], r.radix_items[1], r.radix_ms[1] = 10, 8, 0.1
         r.chosen = _abi.FeTuning(10, 8, 4, 0)
+        r.chosen.nbr_threads[:] = [128, 512, 256, 256]
+        r.chosen.nbr_persistent[:] = [0, 1, 1, 0]
         return r
 
 
@@ -31,11 +34,25 @@ def test_measures_then_reuses(tmp_path):
     d = FakeData()
     r1 = tune(d, path, device="B200|sm148")
     assert r1["source"] == "measured" and d.measured == 1
-    assert r1["tuning"] == {"radix_digit_bits": 10, "radix_items": 8, "mlp_ctas_per_sm": 4}
+    assert r1["tuning"] == {"radix_digit_bits": 10, "radix_items": 8, "mlp_ctas_per_sm": 4,
+                            "nbr_threads": [128, 512, 256, 256],
+                            "nbr_persistent": [0, 1, 1, 0]}
     assert len(r1["report"]["radix"]) == 2
     d2 = FakeData()
     r2 = tune(d2, path, device="B200|sm148")
-    assert r2["source"] == "cache" and d2.measured == 0 and d2.applied == (10, 8, 4)
+    assert r2["source"] == "cache" and d2.measured == 0
+    assert d2.applied == (10, 8, 4, [128, 512, 256, 256], [0, 1, 1, 0])
+
+
+def test_cache_entries_without_neighbour_shapes_apply_the_defaults(tmp_path):
+    path = tmp_path / "old.json"
+    key = cache_key("B200|sm148", FakeData.count, FakeData.table_size, False)
+    path.write_text(json.dumps({key: {"radix_digit_bits": 8, "radix_items": 16,
+                                      "mlp_ctas_per_sm": 3}}))
+    d = FakeData()
+    r = tune(d, str(path), device="B200|sm148")
+    assert r["source"] == "cache"
+    assert d.applied == (8, 16, 3, [256] * 4, [0] * 4)
 
 
 def test_key_separates_classes():
