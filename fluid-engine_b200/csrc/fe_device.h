@@ -77,9 +77,10 @@ struct Bufs {
     float4* pos_a;
     // 32-byte record per particle: pa[2i] = copy of position_b (xyz, written
     // with the whole record by reorder and viscosity), pa[2i+1] = velocity_a,
-    // whose w carries the slot's density from viscosity on (read only by the
-    // learned density source).  The density source fetches a neighbour's
-    // position, velocity and density with one 256-bit load.
+    // whose w carries the slot's density residual t = x / (1 + |x|),
+    // x = 100 (rho / rho0 - 1), from viscosity on (read only by the learned
+    // density source's moments).  The density source fetches a neighbour's
+    // position, velocity and t with one 256-bit load.
     float4* pa;
     // 32-byte record per particle: pv[2i] = copy of position_b (xyz, written
     // by reorder), pv[2i+1] = velocity_b with the slot's density in w

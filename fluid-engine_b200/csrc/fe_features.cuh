@@ -56,12 +56,22 @@ __device__ __forceinline__ uint32_t sample_hash(uint32_t i, uint32_t seed) {
 
 constexpr int kMoments = 5;
 
+// The density residual of one particle as the moments weigh it:
+// t = x / (1 + |x|), x = 100 (rho / rho0 - 1).  It depends on the particle
+// alone, so viscosity stores it once per particle (velocity_a's w) for the
+// learned density source, which gathers it with the velocity.
+__device__ __forceinline__ float density_residual_t(float rho, float rho0) {
+    float x = 100.0f * (rho / rho0 - 1.0f);
+    return x / (1.0f + fabsf(x));
+}
+
 // Running neighbourhood moments of the density residual (orders 1..5).
 struct Moments {
     float w = 0.0f, m[kMoments] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     __device__ __forceinline__ void add(float g, float rho_j, float rho0) {
-        float x = 100.0f * (rho_j / rho0 - 1.0f);
-        float t = x / (1.0f + fabsf(x));
+        add_t(g, density_residual_t(rho_j, rho0));
+    }
+    __device__ __forceinline__ void add_t(float g, float t) {
         float wj = -g;
         w += wj;
         float p = t;

@@ -134,14 +134,15 @@ __global__ void __launch_bounds__(kBlock) k_snapshot4(float4* dst, const float4*
     dst[i] = v;
 }
 
-// pr = p / rho^2 and both velocities' w = rho for all particles (after a
-// host upload of p, rho, position_b or a velocity).
+// pr = p / rho^2, velocity_b's w = rho and velocity_a's w = the density
+// residual t for all particles (after a host upload of p, rho, position_b or
+// a velocity).  One block per chunk (t needs the scene's rho0).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= B.n_total) return;
+    uint32_t i, s, c;
+    if (!chunk_of(B, i, s, c)) return;
     posb(B, i)->w = pressure_over_rho2(B.prs[i], B.rho[i]);
     velb(B, i)->w = B.rho[i];
-    vela(B, i)->w = B.rho[i];
+    vela(B, i)->w = density_residual_t(B.rho[i], B.P[s].rho0);
 }
 
 // ---------------------------------------------------------------------------
@@ -407,10 +408,10 @@ __device__ __forceinline__ void viscosity_particle(const Bufs& B, uint32_t i, ui
     f3 vv = add(vi, scale(P.visc, sum));
     f3 g = {P.gx, P.gy, P.gz};
     f3 vf = add(vv, scale_r(g, P.dt));
-    // the whole position/velocity_a record; w = the slot's density for the
-    // learned density source
+    // the whole position/velocity_a record; w = the slot's density residual
+    // t (density_residual_t) for the learned density source
     st_pair(B.pa, i, make_float4(pi.x, pi.y, pi.z, 0.0f),
-            make_float4(vf.x, vf.y, vf.z, B.rho[i]));
+            make_float4(vf.x, vf.y, vf.z, density_residual_t(B.rho[i], P.rho0)));
 }
 
 template <int kThreads, bool kPersist>
@@ -438,12 +439,12 @@ __device__ __forceinline__ void density_source_body(const Bufs& B, const LearnAr
     const f3 vi = xyz(__ldg(vela(B, i)));
     float div = 0.0f;
     Moments mo;
-    // velocity_a and (w) the density of j from one load of its record
+    // velocity_a and (w) the density residual t of j from one load of its record
     for_each_neighbor_pair(B, P, i, pi, B.pa, [&](f3 rv, float g, float4 vj) {
         f3 grad = scale(g, rv);
         f3 vd = sub(vi, xyz(vj));
         div += m * dot(vd, grad);
-        if (kLearn) mo.add(g, vj.w, P.rho0);
+        if (kLearn) mo.add_t(g, vj.w);   // velocity_a's w: the residual t of j
     });
     float rho_i = B.rho[i];
     float source = 0.0f;
