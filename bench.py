@@ -842,7 +842,7 @@ def run_profile_passes(args) -> None:
     if args.variant == "learned":
         x, y = learned.capture()
         model = learned.train(x, y, epochs=10).model
-        p.warm_start = _abi.FE_WARM_LEARNED
+        p.warm_start = _abi.FE_WARM_LEARNED_DENSITY
     sim = Simulation(w.positions(), p)
     if model is not None:
         _abi.check(sim.data._lib, sim.data._lib.fe_set_model(sim.data.handle, model.handle),
@@ -850,6 +850,8 @@ def run_profile_passes(args) -> None:
     import torch
     for _ in range(3):
         sim.step(1, _abi.FE_STEP_NO_GRAPH)
+    if args.autotune:                        # the shapes the bench runs with
+        sim.data.autotune()
     for _ in range(args.profile_skip):       # further untimed frames (graph replays)
         sim.step(1)
     lib, h = sim.data._lib, sim.data.handle
