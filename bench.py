@@ -652,15 +652,9 @@ def run_gpu(args) -> None:
         model = tr.model
         train_info = {"samples": tr.samples, "val_mse": tr.val_loss,
                       "seconds": time.perf_counter() - t0}
-        # The headline learned arm starts the density solve from the network
-        # (FE_WARM_LEARNED_DENSITY); "learned_both" starts both solves from
-        # it.  At dt = 1 ms the divergence solve needs about one iteration
-        # from the plain start, so its network pass costs more than it saves.
-        for arm, warm in (("learned", _abi.FE_WARM_LEARNED_DENSITY),
-                          ("learned_both", _abi.FE_WARM_LEARNED)):
-            lp = _abi.copy_params(plain_p)
-            lp.warm_start = warm
-            arms[arm] = measure_arm(args, w, lp, model, world, local)
+        lp = _abi.copy_params(plain_p)
+        lp.warm_start = _abi.FE_WARM_LEARNED
+        arms["learned"] = measure_arm(args, w, lp, model, world, local)
     if args.variant in ("plain", "both"):
         arms["plain"] = measure_arm(args, w, plain_p, None, world, local)
     # Whole runs from rest, both arms: the timed window above covers frames
@@ -677,15 +671,11 @@ def run_gpu(args) -> None:
             r = {}
             for arm in arms:
                 pr = _abi.copy_params(wr.params)
-                pr.warm_start = {"learned": _abi.FE_WARM_LEARNED_DENSITY,
-                                 "learned_both": _abi.FE_WARM_LEARNED}.get(
-                                     arm, _abi.FE_WARM_REFERENCE)
-                r[arm] = full_run(wr, pr, model if arm != "plain" else None, local)
-            if "plain" in r and r["plain"]["ms_per_step"]:
-                for arm in ("learned", "learned_both"):
-                    if arm in r and r[arm]["ms_per_step"]:
-                        r[f"{arm}_over_plain"] = (r["plain"]["ms_per_step"]
-                                                  / r[arm]["ms_per_step"])
+                if arm == "learned":
+                    pr.warm_start = _abi.FE_WARM_LEARNED
+                r[arm] = full_run(wr, pr, model if arm == "learned" else None, local)
+            if "learned" in r and "plain" in r and r["plain"]["ms_per_step"]:
+                r["learned_over_plain"] = r["plain"]["ms_per_step"] / r["learned"]["ms_per_step"]
             runs[name] = r
     batch = run_batch(args, world, rank, local) if args.batch else None
     splat = splat_benchmark(w, local) if args.full_runs else None
@@ -732,8 +722,7 @@ def run_gpu(args) -> None:
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(args.workload, w,
                                untimed=args.warmup + (1 if args.autotune else 0))
-        variant = ("learned warm start of the density solve (FE_WARM_LEARNED_DENSITY)"
-                   if "learned" in arms else "plain Jacobi")
+        variant = "learned warm start" if "learned" in arms else "plain Jacobi"
         out = {
             "metric": "DFSPH particle-steps/s (Jacobi to 0.1% density and divergence error)",
             "value": head["value"],
@@ -788,14 +777,6 @@ def run_gpu(args) -> None:
                                                              "divergence": pl["iters"][1]},
                                    "kernel_ms": pl["kern"], "clocks": pl["clocks"]}
             out["learned_over_plain"] = head["value"] / pl["value"]
-            if "learned_both" in arms:
-                lb = arms["learned_both"]
-                out["learned_both_solves"] = {
-                    "value": lb["value"], "ms_per_step": lb["dev_ms"] / args.steps,
-                    "e2e": lb["e2e"],
-                    "avg_jacobi_iterations": {"density": lb["iters"][0],
-                                              "divergence": lb["iters"][1]},
-                    "over_plain": lb["value"] / pl["value"]}
             out["training"] = train_info
         print(json.dumps(out))
     if model is not None:
@@ -842,7 +823,7 @@ def run_profile_passes(args) -> None:
     if args.variant == "learned":
         x, y = learned.capture()
         model = learned.train(x, y, epochs=10).model
-        p.warm_start = _abi.FE_WARM_LEARNED_DENSITY
+        p.warm_start = _abi.FE_WARM_LEARNED
     sim = Simulation(w.positions(), p)
     if model is not None:
         _abi.check(sim.data._lib, sim.data._lib.fe_set_model(sim.data.handle, model.handle),

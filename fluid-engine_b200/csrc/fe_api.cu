@@ -199,7 +199,7 @@ fe_status validate(const fe_params* p) {
             return FE_ERR_INVALID_ARGUMENT;
         }
     if (p->sort_algorithm > FE_SORT_RADIX || p->mode > FE_MODE_FIXED ||
-        p->solver > FE_SOLVER_TOLERANCE || p->warm_start > FE_WARM_LEARNED_DENSITY) {
+        p->solver > FE_SOLVER_TOLERANCE || p->warm_start > FE_WARM_LEARNED) {
         set_error("enum field out of range");
         return FE_ERR_INVALID_ARGUMENT;
     }
@@ -339,9 +339,7 @@ struct fe_ctx {
     uint32_t nbr_persistent[FE_NBR_GROUPS] = {0, 0, 0, 0};
     int num_sms = 148;
 
-    // the network starts the density solve / also the divergence solve
-    bool learned() const { return params[0].warm_start != FE_WARM_REFERENCE && model != nullptr; }
-    bool learned_div() const { return params[0].warm_start == FE_WARM_LEARNED && model != nullptr; }
+    bool learned() const { return params[0].warm_start == FE_WARM_LEARNED && model != nullptr; }
     bool carries() const { return L.carry != nullptr && (learned() || capture); }
 
     uint32_t sort_algorithm() const { return params[0].sort_algorithm; }
@@ -505,10 +503,6 @@ fe_status rec_list_pass(fe_ctx* c, Recorder& R, int pass) {
                 return rec_nbr(c, R, g, NBR_KERNEL(k_density_source_learn, g), c->B, c->L);
             return rec_nbr(c, R, g, NBR_KERNEL(k_density_source, g), c->B);
         default:
-            // the learned variants emit the features the divergence solve's
-            // network reads (or the capture records)
-            if (!(c->learned_div() || c->capture))
-                return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source, g), c->B, fixed);
             if (c->carries() && fixed)
                 return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source_learn_fixed, g), c->B,
                                c->L);
@@ -670,7 +664,7 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     if ((s = rec_neighbor_search(c, R))) return s;
     if ((s = rec_density_alpha(c, R))) return s;
     if ((s = rec_list_pass(c, R, 2))) return s;
-    if (c->learned_div()) {
+    if (c->learned()) {
         if ((s = rec_mlp(c, R))) return s;
         if ((s = rec_trace(c, R, 2 * k + 1))) return s;
         REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 1));
@@ -777,8 +771,7 @@ size_t field_bytes(const fe_ctx* c, fe_field f, void** dptr, size_t* elem, size_
 uint64_t graph_key(const fe_ctx* c, uint32_t n_substeps, bool init) {
     return (uint64_t)n_substeps | ((uint64_t)init << 32) | ((uint64_t)c->sort_algorithm() << 33) |
            ((uint64_t)c->fixed_mode() << 34) | ((uint64_t)c->learned() << 35) |
-           ((uint64_t)c->capture << 36) | ((uint64_t)c->learned_div() << 37) |
-           ((uint64_t)c->trace_slots << 40);
+           ((uint64_t)c->capture << 36) | ((uint64_t)c->trace_slots << 40);
 }
 
 fe_status get_graph(fe_ctx* c, uint32_t n_substeps, bool init, cudaGraphExec_t* out) {
@@ -1620,8 +1613,8 @@ fe_status fe_step(fe_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out)
         set_error("n_substeps %u above 1024", n_substeps);
         return FE_ERR_CAPACITY;
     }
-    if (c->params[0].warm_start != FE_WARM_REFERENCE && !c->model) {
-        set_error("fe_step: a learned warm_start needs a model (fe_set_model)");
+    if (c->params[0].warm_start == FE_WARM_LEARNED && !c->model) {
+        set_error("fe_step: warm_start = FE_WARM_LEARNED needs a model (fe_set_model)");
         return FE_ERR_UNSUPPORTED;
     }
     const bool init = (flags & FE_STEP_INIT_NS) || !c->initialized;

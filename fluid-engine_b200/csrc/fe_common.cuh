@@ -56,31 +56,30 @@ __device__ __forceinline__ float kernel_norm(float h) {
     return 8.0f / (kPi * h3);
 }
 
-// kernel_w (common.glsl:38-54) for q = r / h and k = kernel_norm(h).
+// kernel_w (common.glsl:38-54) for q = r / h and k = kernel_norm(h).  Both
+// pieces of the spline are evaluated, each in the shader's operation order,
+// and the result selected: the same value as the shader's branches (NaN
+// included), without divergent branches in the neighbour loops.
 __device__ __forceinline__ float kernel_w_q(float q, float k) {
-    if (q >= 1.0f) return 0.0f;
-    if (q <= 0.5f) {
-        float q2 = q * q;
-        float q3 = q2 * q;
-        return k * (6.0f * q3 - 6.0f * q2 + 1.0f);
-    } else {
-        float omq = 1.0f - q;
-        float omq3 = omq * omq * omq;
-        return k * 2.0f * omq3;
-    }
+    const float q2 = q * q;
+    const float q3 = q2 * q;
+    const float inner = k * (6.0f * q3 - 6.0f * q2 + 1.0f);
+    const float omq = 1.0f - q;
+    const float omq3 = omq * omq * omq;
+    const float outer = k * 2.0f * omq3;
+    const float w = q <= 0.5f ? inner : outer;
+    return q >= 1.0f ? 0.0f : w;
 }
 
 // kernel_grad (common.glsl:56-73) as the scalar that multiplies r_vec, for
-// q = r / h and k = kernel_norm(h).
+// q = r / h and k = kernel_norm(h); the pieces selected as in kernel_w_q.
+// The division is skipped where the result is 0 (q >= 1 or r < 1e-6).
 __device__ __forceinline__ float kernel_grad_scale_q(float q, float r, float h, float k) {
     if (q >= 1.0f || r < kEpsR) return 0.0f;
-    float gf;
-    if (q <= 0.5f) {
-        gf = k * (18.0f * q * q - 12.0f * q);
-    } else {
-        float omq = 1.0f - q;
-        gf = k * -6.0f * omq * omq;
-    }
+    const float inner = k * (18.0f * q * q - 12.0f * q);
+    const float omq = 1.0f - q;
+    const float outer = k * -6.0f * omq * omq;
+    const float gf = q <= 0.5f ? inner : outer;
     return gf / (h * r);
 }
 

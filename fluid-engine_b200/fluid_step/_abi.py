@@ -47,7 +47,6 @@ FE_SOLVER_TOLERANCE = 1
 # fe_warm_start
 FE_WARM_REFERENCE = 0
 FE_WARM_LEARNED = 1
-FE_WARM_LEARNED_DENSITY = 2
 
 # fe_field
 FE_FIELD_POSITION_A = 0

@@ -93,12 +93,7 @@ typedef enum fe_solver {
 typedef enum fe_warm_start {
     FE_WARM_REFERENCE = 0, /* density solve from 0, divergence solve from the
                               density solve's pressures (as the reference) */
-    FE_WARM_LEARNED = 1,   /* both solves start from the learned MLP κ    */
-    FE_WARM_LEARNED_DENSITY = 2 /* the density solve from the learned κ, the
-                              divergence solve as FE_WARM_REFERENCE: where
-                              the divergence solve needs about one iteration
-                              anyway, its network pass costs more than it
-                              saves */
+    FE_WARM_LEARNED = 1    /* both solves start from the learned MLP κ    */
 } fe_warm_start;
 
 /* ------------------------------------------------------------------------- */

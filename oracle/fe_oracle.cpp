@@ -357,7 +357,6 @@ struct Base {
     // outputs for each solve of the next frame are given (net_out), the
     // features it was fed are kept (rows) for comparison.
     bool learned = false;
-    bool learned_div = false;      // the divergence solve uses the network too
     float norm[28] = {};
     uint32_t net_slots = 0;        // solves with outputs given for the next frame
     std::vector<float> net_out;    // [slot][n][2], standardised outputs
@@ -678,7 +677,7 @@ struct State : Base {
                 }
             });
             src[i] = -div;
-            if (learned_div) emit_row(i, 1, div, vi, mo);
+            if (learned) emit_row(i, 1, div, vi, mo);
         }
     }
 
@@ -1022,7 +1021,7 @@ void substep(Base* s, fe_stats* acc_stats, bool* cap_hit) {
     s->neighbor_search();
     s->density_alpha();
     s->divergence_source();
-    if (s->learned_div) s->warm_apply(1);
+    if (s->learned) s->warm_apply(1);
     uint32_t kd = solve(s, true, &r, cap_hit, &rm);
     acc_stats->divergence_residual_max = rm;
     acc_stats->divergence_iterations = kd;
@@ -1133,11 +1132,10 @@ int fo_step(fo_ctx* c, uint32_t n_substeps, uint32_t flags, fe_stats* out) {
     return 0;
 }
 
-int fo_set_learned(fo_ctx* c, const float* norm28, int divergence_too) {
+int fo_set_learned(fo_ctx* c, const float* norm28) {
     if (!c) return FE_ERR_INVALID_ARGUMENT;
     Base* s = c->s;
     s->learned = norm28 != nullptr;
-    s->learned_div = s->learned && divergence_too != 0;
     if (norm28) std::memcpy(s->norm, norm28, sizeof s->norm);
     s->net_slots = 0;
     return 0;

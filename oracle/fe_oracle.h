@@ -100,10 +100,8 @@ void fo_raymarch(const uint32_t* grid, int rx, int ry, int rz, const float* sky4
  * substep k, 2k + 1 = divergence solve); after it, fo_get_feature_rows
  * returns the BF16 rows rows[n][16] the source passes computed for a slot.
  * fo_learned_missing_outputs: the last fo_step reached a solve without
- * given outputs (its start was left as without the network).
- * divergence_too = 0 restates FE_WARM_LEARNED_DENSITY: only the density
- * solve starts from the network (the odd slots are unused). */
-int fo_set_learned(fo_ctx* ctx, const float* norm28, int divergence_too);
+ * given outputs (its start was left as without the network). */
+int fo_set_learned(fo_ctx* ctx, const float* norm28);
 int fo_set_network_outputs(fo_ctx* ctx, uint32_t slots, const float* out);
 int fo_get_feature_rows(const fo_ctx* ctx, uint32_t slot, uint16_t* rows);
 int fo_learned_missing_outputs(const fo_ctx* ctx);

@@ -56,7 +56,7 @@ def lib():
             "fo_raymarch": (None, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int,
                                    c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
                                    c_void_p]),
-            "fo_set_learned": (c_int, [c_void_p, c_void_p, c_int]),
+            "fo_set_learned": (c_int, [c_void_p, c_void_p]),
             "fo_set_network_outputs": (c_int, [c_void_p, c_uint32, c_void_p]),
             "fo_get_feature_rows": (c_int, [c_void_p, c_uint32, c_void_p]),
             "fo_learned_missing_outputs": (c_int, [c_void_p]),
@@ -153,16 +153,15 @@ class Oracle:
         return out.reshape(count, width) if width == 4 else out
 
     # -- learned warm start (the network's outputs are given, not computed) --
-    def set_learned(self, norm, divergence: bool = True) -> None:
+    def set_learned(self, norm) -> None:
         """Turns the warm start on with the model's standardisation (28
-        floats: x mean[12], x std[12], y mean[2], y std[2]); None: off.
-        divergence=False: the density solve only (FE_WARM_LEARNED_DENSITY)."""
+        floats: x mean[12], x std[12], y mean[2], y std[2]); None: off."""
         if norm is None:
             self._norm = None
-            rc = lib().fo_set_learned(self.h, None, 0)
+            rc = lib().fo_set_learned(self.h, None)
         else:
             self._norm = np.ascontiguousarray(norm[:28], dtype=np.float32)
-            rc = lib().fo_set_learned(self.h, _ptr(self._norm), 1 if divergence else 0)
+            rc = lib().fo_set_learned(self.h, _ptr(self._norm))
         if rc:
             raise RuntimeError(f"oracle set_learned: {rc}")
 

@@ -43,14 +43,13 @@ def random_model():
 
 
 def _learned_frames(oracle_mod, model, name, frames, substeps=1, mode=_abi.FE_MODE_FIXED,
-                    solver=None, n_keep=None, vel_sigma=0.0, warm=_abi.FE_WARM_LEARNED):
+                    solver=None, n_keep=None, vel_sigma=0.0):
     w = scene.workload(name)
     p = _abi.copy_params(w.params)
     p.mode = mode
     if solver is not None:
         p.solver = solver
-    p.warm_start = warm
-    both = warm == _abi.FE_WARM_LEARNED
+    p.warm_start = _abi.FE_WARM_LEARNED
     pos = w.positions()
     if n_keep:
         pos = pos[:n_keep].copy()
@@ -63,14 +62,14 @@ def _learned_frames(oracle_mod, model, name, frames, substeps=1, mode=_abi.FE_MO
     slots = 2 * substeps
     sim.data.trace_learned(slots)
     orc = oracle_mod.Oracle(p, pos, vel)
-    orc.set_learned(model.normalization(), divergence=both)
+    orc.set_learned(model.normalization())
     for f in range(frames):
         st = sim.step(substeps)
         trace = [sim.data.read_trace(k) for k in range(slots)]
         orc.set_network_outputs(np.stack([t[1] for t in trace]))
         rs = orc.step(substeps)
         assert not orc.missing_network_outputs()
-        for k in range(0, slots, 1 if both else 2):   # density-only: even slots
+        for k in range(slots):
             assert_same(trace[k][0], orc.feature_rows(k),
                         f"frame {f}, solve slot {k}: network input rows")
         for s_ in STATS:
@@ -108,10 +107,3 @@ def test_learned_frames_bit_exact_1m(oracle_mod, small_model):
     FIXED mode, tolerance 0.1 %, with an initial velocity field: 2 frames."""
     _learned_frames(oracle_mod, small_model, "dam_break_1m", frames=2, vel_sigma=0.3)
 
-
-def test_density_only_warm_start_bit_exact(oracle_mod, small_model):
-    """FE_WARM_LEARNED_DENSITY: the network starts the density solve only;
-    the divergence solve starts as the plain solver's does."""
-    _learned_frames(oracle_mod, small_model, "dam_break_16k", frames=4,
-                    solver=_abi.FE_SOLVER_TOLERANCE, vel_sigma=0.3,
-                    warm=_abi.FE_WARM_LEARNED_DENSITY)
