@@ -281,18 +281,17 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
             const uint32_t j =
                 __shfl_sync(kFull, start, t) + (cidx - __shfl_sync(kFull, excl, t));
             const float4 q = valid ? __ldg(posb(B, j)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            uint32_t my_mask = 0;
+            // particle p's mask for this slab is the ballot; lane 0 stores it
+#pragma unroll 2
             for (int p = r0; p < r1; ++p) {
                 const float4 a = S.coop.pos[p];
                 const f3 rv = {a.x - q.x, a.y - q.y, a.z - q.z};
                 const float r2 = dot(rv, rv);
                 const uint32_t bits = __ballot_sync(kFull, valid && !(r2 > h2));
-                if (lane == p) my_mask = bits;
+                if (lane == 0) S.coop.mask[sl][p] = bits;
             }
-            if (mine) {
-                S.coop.mask[sl][lane] = my_mask;
-                n_in += __popc(my_mask);
-            }
+            __syncwarp();
+            if (mine) n_in += __popc(S.coop.mask[sl][lane]);
         }
     }
 }
