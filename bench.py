@@ -294,39 +294,50 @@ def measure_arm(args, w, params, model, world, local):
     dev_ms_max = reduce_max(dev_ms, world)
 
     # e2e through the C ABI as a host application drives it, over the same K
-    # frames as the device-timed window (replayed from its start): every frame the
-    # parameter block goes in (sync_with_scene), the frame runs, its stats
-    # come back (the next dt) and its positions are copied out for the
-    # renderer.  The positions' copy (fe_download_async into page-locked
-    # memory, two buffers) overlaps the next frame; the host waits for frame
-    # k's positions after launching frame k+1, and for the last frame's before
-    # the clock stops.
+    # frames as the device-timed window (replayed from its start): every
+    # frame the parameter block goes in (sync_with_scene), the frame runs, its
+    # stats come back and its positions are copied out for the renderer.
+    # Both reads are captured on the device in stream order
+    # (fe_read_stats_async, fe_download_async into page-locked memory, two
+    # buffers) and waited for after the next frame has been launched, so the
+    # GPU never idles on the host; the last frame's are waited for before the
+    # clock stops.  Under adaptive CFL the host's parameter block must carry
+    # the device's latest dt, so there the stats are read before the next
+    # frame is launched.
     sim.data.import_state(window_start)
     del window_start
     p = _abi.copy_params(sim.data.current_params())
     pinned = [torch.empty((n, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
     pos_host = [t.numpy() for t in pinned]
     stats_host = _abi.FeStats()
-    ticket = ctypes.c_uint64()
+    tk_pos, tk_st = ctypes.c_uint64(), ctypes.c_uint64()
+    lagged = not p.use_cfl
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    prev = 0
+    prev = None
     for k in range(args.steps):
         lib.fe_set_params(h, ctypes.byref(p))
         lib.fe_step(h, 1, step_flags, None)
-        lib.fe_read_stats(h, ctypes.byref(stats_host))
+        if lib.fe_read_stats_async(h, ctypes.byref(tk_st)):
+            raise RuntimeError("fe_read_stats_async failed")
         buf = pos_host[k % 2]
-        rc = lib.fe_download_async(h, _abi.FE_FIELD_POSITION_A,
-                                   buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes,
-                                   ctypes.byref(ticket))
-        if rc:
-            raise RuntimeError(f"fe_download_async failed: {rc}")
-        if prev:
-            lib.fe_download_wait(h, prev)
-        prev = ticket.value
-        p.dt = stats_host.dt
-    lib.fe_download_wait(h, prev)
+        if lib.fe_download_async(h, _abi.FE_FIELD_POSITION_A,
+                                 buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes,
+                                 ctypes.byref(tk_pos)):
+            raise RuntimeError("fe_download_async failed")
+        cur = (tk_st.value, tk_pos.value)
+        if not lagged:           # the next parameter block needs this frame's dt
+            lib.fe_stats_wait(h, cur[0], ctypes.byref(stats_host))
+            p.dt = stats_host.dt
+        if prev is not None:     # the previous frame's results, read while this one runs
+            if lagged:
+                lib.fe_stats_wait(h, prev[0], ctypes.byref(stats_host))
+            lib.fe_download_wait(h, prev[1])
+        prev = cur
+    if lagged:
+        lib.fe_stats_wait(h, prev[0], ctypes.byref(stats_host))
+    lib.fe_download_wait(h, prev[1])
     e2e_s = reduce_max(time.perf_counter() - t0, world)
 
     kern = {}
@@ -746,8 +757,9 @@ def run_gpu(args) -> None:
             "e2e": {"value": head["e2e"], "unit": "particle-steps/s",
                     "h2d_bytes_per_step": ctypes.sizeof(_abi.FeParams),
                     "d2h_bytes_per_step": n * 16 + ctypes.sizeof(_abi.FeStats),
-                    "path": "fe_set_params + fe_step + fe_read_stats + fe_download_async("
-                            "position_a, page-locked) overlapping the next frame"},
+                    "path": "fe_set_params + fe_step + fe_read_stats_async + "
+                            "fe_download_async(position_a, page-locked), both waited for "
+                            "while the next frame runs"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,

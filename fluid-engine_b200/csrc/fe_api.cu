@@ -327,6 +327,11 @@ struct fe_ctx {
     void* snap[2] = {nullptr, nullptr};
     size_t snap_cap = 0;
     cudaEvent_t snap_ready[2] = {nullptr, nullptr};
+    // fe_read_stats_async: two mapped host snapshots and their events
+    StatsSnapshot* stats_host = nullptr;     // page-locked, mapped, 2 slots
+    StatsSnapshot* stats_dev = nullptr;      // the same memory as the device sees it
+    cudaEvent_t stats_done[2] = {nullptr, nullptr};
+    uint64_t stats_tickets = 0;
     cudaEvent_t copy_done[2] = {nullptr, nullptr};
     uint64_t tickets = 0;
     uint64_t slot_ticket[2] = {0, 0};
@@ -398,7 +403,9 @@ void release(fe_ctx* c) {
     for (int k = 0; k < 2; ++k) {
         if (c->snap_ready[k]) cudaEventDestroy(c->snap_ready[k]);
         if (c->copy_done[k]) cudaEventDestroy(c->copy_done[k]);
+        if (c->stats_done[k]) cudaEventDestroy(c->stats_done[k]);
     }
+    if (c->stats_host) cudaFreeHost(c->stats_host);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -809,24 +816,18 @@ fe_status get_graph(fe_ctx* c, uint32_t n_substeps, bool init, cudaGraphExec_t* 
     return FE_OK;
 }
 
-fe_status collect_stats(fe_ctx* c, fe_stats* out, uint32_t scene = 0) {
-    FE_CUDA(cudaMemcpyAsync(c->h_state + scene, c->B.S + scene, sizeof(SceneState),
-                            cudaMemcpyDeviceToHost, c->stream));
-    FE_CUDA(cudaMemcpyAsync(c->h_global, c->B.G, sizeof(GlobalState), cudaMemcpyDeviceToHost,
-                            c->stream));
-    DevParams dp;
-    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P + scene, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
-    FE_CUDA(cudaStreamSynchronize(c->stream));
-    const SceneState& S = c->h_state[scene];
+// fe_stats of one scene from its device state, the global flags and its dt.
+void stats_from(const fe_ctx* c, const SceneState& S, const GlobalState& G, float dt, uint32_t n_p,
+                fe_stats* out) {
     std::memset(out, 0, sizeof *out);
     out->max_speed_bits = S.stats[0];
     out->density_error_fp = S.stats[1];
     out->divergence_error_fp = S.stats[2];
     std::memcpy(&out->max_speed, &S.stats[0], 4);
-    float n = (float)dp.n;
+    float n = (float)n_p;
     out->avg_density_error = (float)S.stats[1] / (1.0f * n);
     out->avg_divergence_error = (float)S.stats[2] / (10.0f * n);
-    out->dt = dp.dt;
+    out->dt = dt;
     out->avg_density_error_f64 = S.stats_f64[0];
     out->avg_divergence_error_f64 = S.stats_f64[1];
     out->density_residual = S.last_metric[0];
@@ -838,13 +839,25 @@ fe_status collect_stats(fe_ctx* c, fe_stats* out, uint32_t scene = 0) {
     out->total_density_iterations = S.total_iters[0];
     out->total_divergence_iterations = S.total_iters[1];
     out->substeps = c->last_substeps;
-    uint32_t flags = c->h_global->flags;  // cap hit and look-back timeout: any scene
+    uint32_t flags = G.flags;  // cap hit and look-back timeout: any scene
     if (S.nonfinite) flags |= 0x8u;
     out->flags = flags;
+}
+
+fe_status collect_stats(fe_ctx* c, fe_stats* out, uint32_t scene = 0) {
+    FE_CUDA(cudaMemcpyAsync(c->h_state + scene, c->B.S + scene, sizeof(SceneState),
+                            cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaMemcpyAsync(c->h_global, c->B.G, sizeof(GlobalState), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DevParams dp;
+    FE_CUDA(cudaMemcpyAsync(&dp, c->B.P + scene, sizeof dp, cudaMemcpyDeviceToHost, c->stream));
+    FE_CUDA(cudaStreamSynchronize(c->stream));
+    stats_from(c, c->h_state[scene], *c->h_global, dp.dt, dp.n, out);
     // host-side mirror of the device dt
     c->params[scene].dt = dp.dt;
     return FE_OK;
 }
+
 
 }  // namespace
 
@@ -1590,6 +1603,49 @@ fe_status fe_read_stats(fe_ctx* c, fe_stats* out) {
     }
     FE_CUDA(cudaSetDevice(c->device));
     return collect_stats(c, out);
+}
+
+fe_status fe_read_stats_async(fe_ctx* c, uint64_t* ticket) {
+    if (!c || !ticket) {
+        set_error("NULL argument");
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    if (!c->stats_host) {
+        FE_CUDA(cudaHostAlloc(&c->stats_host, 2 * sizeof(StatsSnapshot), cudaHostAllocMapped));
+        FE_CUDA(cudaHostGetDevicePointer((void**)&c->stats_dev, c->stats_host, 0));
+        for (int k = 0; k < 2; ++k)
+            FE_CUDA(cudaEventCreateWithFlags(&c->stats_done[k], cudaEventDisableTiming));
+    }
+    const uint64_t t = ++c->stats_tickets;
+    const int slot = (int)(t & 1u);
+    Recorder R = eager(c);
+    REC(R.k(k_stats_snapshot, dim3(1), dim3(32), c->B, c->stats_dev + slot, 0u));
+    FE_CUDA(cudaEventRecord(c->stats_done[slot], c->stream));
+    *ticket = t;
+    return FE_OK;
+}
+
+fe_status fe_stats_wait(fe_ctx* c, uint64_t ticket, fe_stats* out) {
+    if (!c || !out || ticket == 0 || ticket > c->stats_tickets || ticket + 2 <= c->stats_tickets) {
+        set_error("fe_stats_wait: unknown or overwritten ticket %llu",
+                  (unsigned long long)ticket);
+        return FE_ERR_INVALID_ARGUMENT;
+    }
+    FE_CUDA(cudaSetDevice(c->device));
+    const int slot = (int)(ticket & 1u);
+    FE_CUDA(cudaEventSynchronize(c->stats_done[slot]));
+    const StatsSnapshot& snap = c->stats_host[slot];
+    stats_from(c, snap.S, snap.G, snap.dt, snap.n, out);
+    if (out->flags & 0x4u) {
+        set_error("a bounded device wait timed out (look-back)");
+        return FE_ERR_TIMEOUT;
+    }
+    if (out->flags & 0x8u) {
+        set_error("non-finite velocity, density or source term in the stats pass");
+        return FE_ERR_NON_FINITE;
+    }
+    return FE_OK;
 }
 
 fe_status fe_read_scene_stats(fe_ctx* c, uint32_t scene, fe_stats* out) {
@@ -2435,8 +2491,14 @@ FE_API fe_status fe_state_import(fe_ctx* c, const void* src, size_t bytes) {
     }
     FE_CUDA(cudaSetDevice(c->device));
     fe_status s = FE_OK;
+    const bool had_carry = c->L.carry != nullptr;
     if (carry && (s = ensure_learn_buffers(c)) != FE_OK) return s;
-    drop_graphs(c);
+    // Recorded frame graphs stay valid: they reach the state through the
+    // same device buffers, and their key covers everything the snapshot can
+    // change in a frame's structure (first frame, mode, sort, warm start).
+    // Only new learned-state buffers make them stale.
+    if (!had_carry && c->L.carry) drop_graphs(c);
+    FE_CUDA(cudaStreamSynchronize(c->stream));
     const char* p = dev_params;
     const char* global = nullptr;
     for (const Section& sec : state_sections(c, carry)) {

@@ -72,6 +72,15 @@ struct GlobalState {
 
 enum Ticket : int { kTicketStats = 0, kTicketSolve = 1, kTicketHist = 2 };
 
+// The stats of one scene as fe_read_stats_async captures them (written by
+// k_stats_snapshot into page-locked, device-mapped host memory).
+struct StatsSnapshot {
+    SceneState S;
+    GlobalState G;
+    float dt;
+    uint32_t n;
+};
+
 // Kernel-side view of every buffer of a context (passed by value).
 struct Bufs {
     float4* pos_a;

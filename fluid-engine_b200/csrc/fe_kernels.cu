@@ -1003,6 +1003,18 @@ __global__ void k_frame_prologue(Bufs B) {
     S.iters_div = (early && avg_ve < thr_v) ? 1u : P.k_div;
 }
 
+// fe_read_stats_async: scene `scene`'s stats, the global flags and its dt,
+// in stream order, into mapped host memory (one thread; a few hundred
+// bytes).
+__global__ void k_stats_snapshot(Bufs B, StatsSnapshot* dst, uint32_t scene) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    dst->S = B.S[scene];
+    dst->G = *B.G;
+    dst->dt = B.P[scene].dt;
+    dst->n = B.P[scene].n;
+    __threadfence_system();
+}
+
 __global__ void k_count_substep(Bufs B) {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < B.n_scenes) B.S[s].substeps += 1;

@@ -339,6 +339,8 @@ SIGNATURES = {
     "fe_download": (c_int, [CTX, c_int, c_void_p, c_size_t]),
     "fe_download_async": (c_int, [CTX, c_int, c_void_p, c_size_t, POINTER(ctypes.c_uint64)]),
     "fe_download_wait": (c_int, [CTX, ctypes.c_uint64]),
+    "fe_read_stats_async": (c_int, [CTX, POINTER(ctypes.c_uint64)]),
+    "fe_stats_wait": (c_int, [CTX, ctypes.c_uint64, POINTER(FeStats)]),
     "fe_neighbor_search": (c_int, [CTX]),
     "fe_density_alpha": (c_int, [CTX]),
     "fe_viscosity": (c_int, [CTX]),

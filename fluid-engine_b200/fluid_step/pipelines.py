@@ -84,6 +84,20 @@ class GpuPhysicsData:
             ctypes.byref(t)), "fe_download_async")
         return int(t.value)
 
+    def read_stats_async(self) -> int:
+        """Captures the last stats pass's stats without waiting; the ticket
+        goes to stats_wait."""
+        t = ctypes.c_uint64()
+        check(self._lib, self._lib.fe_read_stats_async(self.handle, ctypes.byref(t)),
+              "fe_read_stats_async")
+        return int(t.value)
+
+    def stats_wait(self, ticket: int) -> _abi.FeStats:
+        st = _abi.FeStats()
+        check(self._lib, self._lib.fe_stats_wait(self.handle, ticket, ctypes.byref(st)),
+              "fe_stats_wait")
+        return st
+
     def download_wait(self, ticket: int) -> None:
         check(self._lib, self._lib.fe_download_wait(self.handle, ticket), "fe_download_wait")
 

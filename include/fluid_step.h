@@ -360,6 +360,16 @@ FE_API fe_status fe_raymarch(fe_ctx* ctx, const fe_camera* camera);
 /* Reads the stats of the last stats pass (host read of `stats_buffer`,
  * renderer/mod.rs:231-236).  Synchronises the context's stream. */
 FE_API fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
+/* The same read without waiting.  The stats of the last stats pass (scene 0)
+ * are captured on the device in the context's stream order, into
+ * page-locked host memory the library owns, so fe_step calls made right
+ * after run at once; fe_stats_wait(ticket) waits for the capture and fills
+ * `out` (with the same FE_ERR_TIMEOUT / FE_ERR_NON_FINITE results as
+ * fe_step).  A host loop can so read frame k's stats while frame k+1 runs
+ * (the device keeps dt itself under adaptive CFL).  Two captures rotate: a
+ * ticket can be waited for until the capture two after it starts. */
+FE_API fe_status fe_read_stats_async(fe_ctx* ctx, uint64_t* ticket);
+FE_API fe_status fe_stats_wait(fe_ctx* ctx, uint64_t ticket, fe_stats* out);
 /* The stats of one scene of a batch (fe_read_stats reads scene 0).  The
  * FE_STATS_ITERATION_CAP_HIT and look-back flags are shared by all scenes. */
 FE_API fe_status fe_read_scene_stats(fe_ctx* ctx, uint32_t scene, fe_stats* out);

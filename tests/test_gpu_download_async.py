@@ -55,3 +55,37 @@ def test_async_download_into_pageable_memory_and_bad_tickets():
     assert d._lib.fe_download_wait(d.handle, t + 5) == _abi.FE_ERR_INVALID_ARGUMENT
     assert d._lib.fe_download_wait(d.handle, 0) == _abi.FE_ERR_INVALID_ARGUMENT
     sim.close()
+
+
+def test_async_stats_equal_the_waiting_read_across_frames():
+    """fe_read_stats_async captures a frame's stats in stream order: waited
+    for a frame later, they equal what fe_step returned for that frame."""
+    w = scene.workload("dam_break_16k")
+    p = _abi.copy_params(w.params)
+    p.mode, p.solver, p.use_cfl, p.dt = (_abi.FE_MODE_FIXED, _abi.FE_SOLVER_TOLERANCE, 1, 0.004)
+    ref = Simulation(w.positions()[:8000], p)
+    sim = Simulation(w.positions()[:8000], p)
+    lib, h = sim.data._lib, sim.data.handle
+    expect, tickets = [], []
+    for _ in range(6):
+        expect.append(ref.step(1))
+        assert lib.fe_step(h, 1, 0, None) == 0
+        tickets.append(sim.data.read_stats_async())
+        if len(tickets) >= 2:   # the previous frame's capture, a frame later
+            got = sim.data.stats_wait(tickets[-2])
+            _same_stats(got, expect[-2])
+    _same_stats(sim.data.stats_wait(tickets[-1]), expect[-1])
+    assert lib.fe_stats_wait(h, tickets[-3], None) == _abi.FE_ERR_INVALID_ARGUMENT
+    bad = _abi.FeStats()
+    import ctypes
+    assert lib.fe_stats_wait(h, tickets[-3], ctypes.byref(bad)) == _abi.FE_ERR_INVALID_ARGUMENT
+    ref.close()
+    sim.close()
+
+
+def _same_stats(a, b):
+    for name, _ in _abi.FeStats._fields_:
+        if name in ("reserved",):
+            continue
+        va, vb = getattr(a, name), getattr(b, name)
+        assert va == vb or (va != va and vb != vb), (name, va, vb)
