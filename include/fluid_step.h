@@ -297,7 +297,9 @@ FE_API fe_status fe_download(fe_ctx* ctx, fe_field field, void* dst, size_t byte
  * valid, and should be page-locked (cudaHostAlloc, cudaHostRegister) for the
  * copy to overlap; it holds the field, with the reference's w as fe_download
  * gives it, once fe_download_wait(ticket) returns.  Two snapshots rotate:
- * a third fe_download_async waits, on the device, for the copy of the first. */
+ * a third fe_download_async waits, on the device, for the copy of the first.
+ * The first call on a context allocates its two device snapshots and a copy
+ * stream (and a larger field later reallocates them): make it at start-up. */
 FE_API fe_status fe_download_async(fe_ctx* ctx, fe_field field, void* dst, size_t bytes,
                                    uint64_t* ticket);
 FE_API fe_status fe_download_wait(fe_ctx* ctx, uint64_t ticket);
@@ -367,7 +369,8 @@ FE_API fe_status fe_read_stats(fe_ctx* ctx, fe_stats* out);
  * `out` (with the same FE_ERR_TIMEOUT / FE_ERR_NON_FINITE results as
  * fe_step).  A host loop can so read frame k's stats while frame k+1 runs
  * (the device keeps dt itself under adaptive CFL).  Two captures rotate: a
- * ticket can be waited for until the capture two after it starts. */
+ * ticket can be waited for until the capture two after it starts.  The first
+ * call on a context allocates the page-locked capture memory. */
 FE_API fe_status fe_read_stats_async(fe_ctx* ctx, uint64_t* ticket);
 FE_API fe_status fe_stats_wait(fe_ctx* ctx, uint64_t ticket, fe_stats* out);
 /* The stats of one scene of a batch (fe_read_stats reads scene 0).  The
