@@ -234,9 +234,10 @@ def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = Fal
     fixed = 1 + 1 + 4 + 1 + 1 + 1 + 1 + 1
     # per Jacobi iteration: force, update, loop guard
     iters = 3 * (stats.density_iterations + stats.divergence_iterations)
-    # learned: 2 x (network, apply); features, after-solve bookkeeping and the
-    # carry permutation ride in the source, integration and reorder passes
-    extra = 4 if learned else 0
+    # learned: 2 x the network (which also applies the start); features,
+    # after-solve bookkeeping and the carry permutation ride in the source,
+    # integration and reorder passes
+    extra = 2 if learned else 0
     return 1 + ns + fixed + iters + extra + 1   # + prologue, stats
 
 

@@ -623,18 +623,18 @@ fe_status rec_solve(fe_ctx* c, Recorder& R, int which) {
     return FE_OK;
 }
 
-// Network inference on the feature rows (tensor-core kernel of fe_mlp.cu).
-fe_status rec_mlp(fe_ctx* c, Recorder& R) {
+// Network inference on the feature rows (tensor-core kernel of fe_mlp.cu),
+// which also starts solve `which` from its output (warm_apply_particle).
+fe_status rec_mlp(fe_ctx* c, Recorder& R, int which) {
     mlp::KernelLaunch KL;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    REC(mlp::infer_launch(c->n, sms, &KL, c->mlp_ctas));
+    REC(mlp::infer_launch(c->n, c->num_sms, &KL, c->mlp_ctas, true));
     mlp::Params P = c->model->params();
     const __nv_bfloat16* X = static_cast<const __nv_bfloat16*>(c->L.xb);
     float* out = c->L.out;
     uint32_t n = c->n;
     uint32_t* flags = &c->B.G->flags;
-    void* args[] = {&P, &X, &out, &n, &flags};
+    mlp::ApplyArgs A{c->B, c->L, which};
+    void* args[] = {&P, &X, &out, &n, &flags, &A};
     REC(R.launch(KL.func, KL.grid, KL.block, KL.smem, args));
     return FE_OK;
 }
@@ -658,10 +658,9 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     fe_status s;
     if ((s = rec_list_pass(c, R, 0))) return s;
     if ((s = rec_list_pass(c, R, 1))) return s;
-    if (c->learned()) {
-        if ((s = rec_mlp(c, R))) return s;
+    if (c->learned()) {   // the network, which also starts the density solve
+        if ((s = rec_mlp(c, R, 0))) return s;
         if ((s = rec_trace(c, R, 2 * k))) return s;
-        REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 0));
     }
     if ((s = rec_solve(c, R, 0))) return s;
     if (c->carries())
@@ -671,10 +670,9 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     if ((s = rec_neighbor_search(c, R))) return s;
     if ((s = rec_density_alpha(c, R))) return s;
     if ((s = rec_list_pass(c, R, 2))) return s;
-    if (c->learned()) {
-        if ((s = rec_mlp(c, R))) return s;
+    if (c->learned()) {   // ... and the divergence solve
+        if ((s = rec_mlp(c, R, 1))) return s;
         if ((s = rec_trace(c, R, 2 * k + 1))) return s;
-        REC(R.k(k_warm_apply, chunk_grid(c), dim3(kBlock), B, c->L, 1));
     }
     if ((s = rec_solve(c, R, 1))) return s;
     if (c->carries())

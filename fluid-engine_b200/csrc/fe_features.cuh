@@ -136,6 +136,73 @@ __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
     L.carry[i].w = __uint_as_float(slot);
 }
 
+// Applies the network's pressure to the solve about to start (output
+// `which`, in normalised units, rescaled with the current state).  Output 0
+// is the density solve's kappa; output 1 is the divergence solve's kappa
+// minus the density kappa of this substep (the start the divergence solve
+// takes without the network, divergence_source_term.comp leaving p alone).
+//
+// The start is clamped from above.  With p1 = max(omega s_i / a_ii, 0) the
+// first Jacobi iterate from zero, d_i = p1 / omega is the pressure that
+// resolves particle i's source on its own (neighbours at zero pressure).  The
+// density start is at most max(d_i, kappa_d,prev) (the particle's density
+// kappa of the previous substep); the divergence start at most
+// max(d_i, kappa_d) (this substep's density kappa, the start without the
+// network).  scale_i grows as 1/alpha_i, so without a bound a small error of
+// the network at a particle with few neighbours becomes a pressure far above
+// anything the plain solver produces there, which the mean tolerance metric
+// cannot see and which throws particles out at 10^4 m/s within a few hundred
+// frames.  A bound that includes the previous divergence kappa, or a factor
+// above 1, feeds such errors back from substep to substep and is not stable
+// either.  Under the bound the start stays near or below the solution,
+// where Jacobi approaches from the same side as the plain solver.
+//
+// Particles with fewer than kMinNeighbours neighbours (the free surface and
+// splashes, where alpha is small, scale_i large and training samples few)
+// keep the plain start.  Without this, a long adaptive-CFL run of the 262k
+// dam break still threw single particles out at 10^2 - 10^3 m/s late in the
+// run (a few over-pressured particles do not move the mean tolerance); with
+// it the largest speed matches the plain solver's.
+constexpr uint32_t kMinNeighbours = 16;
+// y_std: the network's output `which` for particle i in standardised units.
+__device__ __forceinline__ void warm_apply_particle(const Bufs& B, const LearnArgs& L,
+                                                    const DevParams& P, uint32_t i, int which,
+                                                    float y_std) {
+    const float rho = B.rho[i], alpha = B.alpha[i];
+    const float scale = kappa_scale(rho, alpha, P.dt, P.rho0);
+    const float y = y_std * L.norm[26 + which] + L.norm[24 + which];
+    const float4 carry = L.carry[i];
+    const float base = which == 1 ? carry.x : 0.0f;
+    // Comparisons rather than fminf/fmaxf, so that no signed zero depends on
+    // how a maximum of -0 and +0 is taken: every value below is +0 or
+    // positive, and NaN becomes 0.
+    float p1 = 0.0f;
+    if (alpha > kEpsR && rho > kEpsR) {
+        const float a_ii = -(P.dt / (rho * rho)) * alpha;
+        if (fabsf(a_ii) > 1e-20f) {
+            const float q = (P.omega * B.src[i]) / a_ii;
+            p1 = q > 0.0f ? q : 0.0f;
+        }
+    }
+    const float d = p1 / P.omega;
+    float p = B.nbr_count[i] < kMinNeighbours ? base : base + y * scale;
+    p = p > 0.0f ? p : 0.0f;  // NaN -> 0; pressures are clamped at 0 as in pressure_update
+    const float bound = d > carry.x ? d : carry.x;
+    p = p < bound ? p : bound;
+    B.prs[i] = p;
+    posb(B, i)->w = pressure_over_rho2(p, rho);
+}
+
+// The scene of particle g (scenes are laid out back to back).
+__device__ __forceinline__ uint32_t scene_of(const Bufs& B, uint32_t g) {
+    uint32_t lo = 0, hi = B.n_scenes;   // first scene whose first particle is > g, minus one
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (B.P[mid].first <= g) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // After solve `which`: the final pressure becomes the particle's "last kappa"
 // and, in capture mode, the training target of its sample slot (for the
 // divergence solve relative to the substep's density kappa, as the warm start

@@ -55,7 +55,6 @@ template <int kThreads, bool kPersist>
 __global__ void k_divergence_source_learn(Bufs B, int fixed, LearnArgs L);
 template <int kThreads, bool kPersist>
 __global__ void k_divergence_source_learn_fixed(Bufs B, LearnArgs L);
-__global__ void k_warm_apply(Bufs B, LearnArgs L, int which);
 __global__ void k_carry_take(Bufs B, LearnArgs L);
 __global__ void k_stats_snapshot(Bufs B, StatsSnapshot* dst, uint32_t scene);
 __global__ void k_snapshot4(float4* dst, const float4* src, uint32_t stride, uint32_t n,

@@ -19,6 +19,7 @@
 
 #include <cstdint>
 
+#include "fe_features.cuh"
 #include "fe_mlp.h"
 
 namespace fe {
@@ -268,10 +269,11 @@ __device__ __forceinline__ void epilogue_half(uint32_t taddr, uint32_t c0, const
     }
 }
 
+template <bool kApply>
 __global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
                                                              const __nv_bfloat16* __restrict__ X,
                                                              float* __restrict__ out, uint32_t n,
-                                                             uint32_t* error_flags) {
+                                                             uint32_t* error_flags, ApplyArgs A) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
     const uint32_t tid = threadIdx.x;
@@ -356,8 +358,15 @@ __global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
             float v[16];
             tmem_ld16(lane_addr8(d, 0), v);
             const uint32_t g = tile * kTile + row;
-            if (g < n)
-                reinterpret_cast<float2*>(out)[g] = make_float2(v[0] + S.W.b3[0], v[1] + S.W.b3[1]);
+            if (g < n) {
+                const float o0 = v[0] + S.W.b3[0], o1 = v[1] + S.W.b3[1];
+                reinterpret_cast<float2*>(out)[g] = make_float2(o0, o1);
+                // the solve's start from this output (the same value the
+                // stand-alone pass would read back from `out`)
+                if (kApply)
+                    warm_apply_particle(A.B, A.L, A.B.P[scene_of(A.B, g)], g, A.which,
+                                        A.which == 0 ? o0 : o1);
+            }
         }
         tc_before_sync();
         __syncthreads();
@@ -663,16 +672,18 @@ __global__ void k_adam(float* __restrict__ master, float* __restrict__ grad, flo
 size_t infer_smem_bytes() { return sizeof(InferSmem) + 1024; }
 size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
 
-cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out, int ctas_per_sm) {
+cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out, int ctas_per_sm,
+                         bool apply) {
     size_t smem = infer_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const void* func = apply ? (const void*)k_mlp_infer<true> : (const void*)k_mlp_infer<false>;
+    cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     if (ctas_per_sm < 1 || ctas_per_sm > kInferMaxCtasPerSm) return cudaErrorInvalidValue;
     uint32_t tiles = (n + kTile - 1) / kTile;
     const uint32_t cap = (uint32_t)(num_sms * ctas_per_sm);
     uint32_t grid = tiles < cap ? tiles : cap;
-    out->func = (const void*)k_mlp_infer;
+    out->func = func;
     out->grid = dim3(grid > 0 ? grid : 1);
     out->block = dim3(kInferThreads);
     out->smem = smem;
@@ -685,7 +696,8 @@ cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t 
     KernelLaunch L;
     cudaError_t e = infer_launch(n, num_sms, &L, ctas_per_sm);
     if (e != cudaSuccess) return e;
-    k_mlp_infer<<<L.grid, L.block, L.smem, stream>>>(P, X, out, n, error_flags);
+    k_mlp_infer<false><<<L.grid, L.block, L.smem, stream>>>(P, X, out, n, error_flags,
+                                                            ApplyArgs{});
     return cudaGetLastError();
 }
 

@@ -7,6 +7,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "fe_device.h"
+
 namespace fe {
 namespace mlp {
 
@@ -40,9 +42,19 @@ __host__ __device__ inline Grads grads_from(float* g, float* loss) {
 
 size_t infer_smem_bytes();
 
+// What the inference kernel needs to start a solve from its output in the
+// same pass (the warm start of fe_features.cuh, warm_apply_particle):
+// output `which` of particle g becomes its initial pressure.
+struct ApplyArgs {
+    Bufs B;
+    LearnArgs L;
+    int which;
+};
+
 // The inference kernel as a launch description (for CUDA-graph recording):
 // arguments (Params, const __nv_bfloat16* X, float* out, uint32_t n,
-// uint32_t* error_flags).  Sets the kernel's shared-memory attribute.
+// uint32_t* error_flags, ApplyArgs).  With `apply` the kernel also starts
+// solve A.which from its output.  Sets the kernel's shared-memory attribute.
 struct KernelLaunch {
     const void* func;
     dim3 grid, block;
@@ -54,7 +66,7 @@ struct KernelLaunch {
 constexpr int kInferDefaultCtasPerSm = 6;
 constexpr int kInferMaxCtasPerSm = 6;
 cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out,
-                         int ctas_per_sm = kInferDefaultCtasPerSm);
+                         int ctas_per_sm = kInferDefaultCtasPerSm, bool apply = false);
 size_t train_smem_bytes();
 
 // out[i][0..1] for the BF16 rows X[i][0..15], i < n.
