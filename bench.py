@@ -230,8 +230,9 @@ def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = Fal
     ns = 1 + 1 + 1 + passes + 1 + 1 + 1 + (1 if fixed_mode else 0) + \
         (1 if learned and not fixed_mode else 0)
     # viscosity, density source, 2 x (solve begin + end), integration, density/alpha,
-    # divergence source, divergence integration, substep counter
-    fixed = 1 + 1 + 4 + 1 + 1 + 1 + 1 + 1
+    # divergence source (plain: summed inside density/alpha), divergence
+    # integration, substep counter
+    fixed = 1 + 1 + 4 + 1 + 1 + (1 if learned else 0) + 1 + 1
     # per Jacobi iteration: force, update, loop guard
     iters = 3 * (stats.density_iterations + stats.divergence_iterations)
     # learned: 2 x the network (which also applies the start); features,
@@ -664,11 +665,12 @@ def run_gpu(args) -> None:
     model = None
     train_info = None
     if args.variant in ("learned", "both"):
-        # The network is trained here, before any timing, on pairs captured
-        # from the plain solver on the 16k and 262k dam breaks.
+        # The network is trained here, before any timing: on pairs captured
+        # from the plain solver on the 16k and 262k dam breaks, then on those
+        # and the same scenes captured under the first network's warm start
+        # (learned.train_on_own_starts).
         t0 = time.perf_counter()
-        x, y = learned.capture(device=local)
-        tr = learned.train(x, y, epochs=30, device=local)
+        tr = learned.train_on_own_starts(epochs=30, device=local)
         model = tr.model
         train_info = {"samples": tr.samples, "val_mse": tr.val_loss,
                       "seconds": time.perf_counter() - t0}

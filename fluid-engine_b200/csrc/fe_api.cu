@@ -481,6 +481,20 @@ fe_status rec_density_alpha(fe_ctx* c, Recorder& R) {
                    c->B);
 }
 
+// density_alpha that also sums the plain divergence source (the mid-substep
+// neighbour search's pass, when no learned state rides along).
+fe_status rec_density_alpha_div(fe_ctx* c, Recorder& R) {
+    const int g = FE_NBR_DENSITY_ALPHA;
+    const uint32_t t = c->nbr_threads[g];
+    return rec_nbr(c, R, g,
+                   c->nbr_persistent[g]
+                       ? pick(k_density_alpha_div<128, true>, k_density_alpha_div<256, true>,
+                              k_density_alpha_div<256, true>, t)
+                       : pick(k_density_alpha_div<128, false>, k_density_alpha_div<256, false>,
+                              k_density_alpha_div<256, false>, t),
+                   c->B, c->fixed_mode() ? 1 : 0);
+}
+
 // Whether a shape may run group g.
 bool nbr_shape_ok(int g, uint32_t threads, uint32_t persistent) {
     if (persistent > 1) return false;
@@ -668,8 +682,12 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     else if ((s = rec_simple(c, R, k_pressure_integration)))
         return s;
     if ((s = rec_neighbor_search(c, R))) return s;
-    if ((s = rec_density_alpha(c, R))) return s;
-    if ((s = rec_list_pass(c, R, 2))) return s;
+    if (c->carries()) {   // the learned source needs this pass's densities
+        if ((s = rec_density_alpha(c, R))) return s;
+        if ((s = rec_list_pass(c, R, 2))) return s;
+    } else if ((s = rec_density_alpha_div(c, R))) {
+        return s;
+    }
     if (c->learned()) {   // ... and the divergence solve
         if ((s = rec_mlp(c, R, 1))) return s;
         if ((s = rec_trace(c, R, 2 * k + 1))) return s;

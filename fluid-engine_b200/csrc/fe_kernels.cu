@@ -194,12 +194,16 @@ struct DensityAcc {
     float density = 0.0f, sum_grad_sq = 0.0f;
     f3 grad_sum = {0.0f, 0.0f, 0.0f};
     uint32_t cnt = 0;
+    float div = 0.0f;   // kDiv: the divergence source's sum
 };
 
-// kn = kernel_norm(h); q = r / h is shared by W and grad W.
+// kn = kernel_norm(h); q = r / h is shared by W and grad W.  kDiv != 0 also
+// sums divergence_source_term.comp's m (v_i - v_j) . grad W over the same
+// pairs in the same order (vi, vj: the velocities that pass binds).
+template <int kDiv>
 __device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, float kn,
                                              uint32_t j, f3 rv, float r2, uint2* out,
-                                             uint32_t stride) {
+                                             uint32_t stride, f3 vi, float4 vj) {
     float r = sqrtf(r2);
     float q = r / h;
     float w = kernel_w_q(q, kn);
@@ -210,9 +214,24 @@ __device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, fl
         f3 mg = scale(m, grad);
         a.grad_sum = add(a.grad_sum, mg);
         a.sum_grad_sq += dot(mg, mg);
+        if (kDiv) {
+            f3 vd = sub(vi, xyz(vj));
+            a.div += m * dot(vd, grad);
+        }
         if (a.cnt < kNbrCap) out[(size_t)a.cnt * stride] = make_uint2(j, __float_as_uint(g));
         ++a.cnt;
     }
+}
+
+// Neighbour j's position (and, kDiv, the velocity the fused divergence
+// source binds: velocity_b's record in FIXED mode, velocity_a's in
+// REFERENCE mode; both records start with a copy of position_b).
+template <int kDiv>
+__device__ __forceinline__ f3 neighbour_pos(const Bufs& B, uint32_t j, float4& vj) {
+    if (kDiv == 0) return xyz(__ldg(posb(B, j)));
+    float4 q;
+    ld_pair(kDiv == 1 ? B.pv : B.pa, j, q, vj);
+    return xyz(q);
 }
 
 // Cooperative phase 1 over the runs of one warp (see above).  Returns, for
@@ -301,6 +320,10 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
 template <int kThreads>
 constexpr int kMinBlocks = 1024 / kThreads;
 
+// kDiv: 0 density and alpha only; 1 also the FIXED-mode divergence source
+// (velocity_b), 2 also the REFERENCE-mode one (velocity_a) -- see
+// density_term.
+template <int kDiv>
 __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScratch& S,
                                                        uint32_t i, uint32_t s, bool live) {
     const DevParams& P = B.P[s];
@@ -336,6 +359,8 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     uint2* out = B.nbr + i;
     const uint32_t stride = B.n_total;
     DensityAcc a;
+    const f3 vi = kDiv ? xyz(__ldg(kDiv == 1 ? velb(B, i) : vela(B, i))) : f3{0.0f, 0.0f, 0.0f};
+    float4 vj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (coop && my_table >= 0) {
         const RunTable& T = S.coop.table[my_table];
         uint32_t sl = 0, bits = S.coop.mask[0][lane];
@@ -351,20 +376,22 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
                 next_excl = T.excl[t + 1];
             }
             const uint32_t j = cur_start + (cidx - cur_excl);
-            f3 rv = sub(pi, xyz(__ldg(posb(B, j))));
-            density_term(a, m, h, kn, j, rv, dot(rv, rv), out, stride);
+            f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
+            density_term<kDiv>(a, m, h, kn, j, rv, dot(rv, rv), out, stride, vi, vj);
         }
     } else if (!coop && n1 <= (uint32_t)kStage) {
         for (uint32_t k = 0; k < n1; ++k) {
             uint32_t j = S.cand[k][lane];
-            f3 rv = sub(pi, xyz(__ldg(posb(B, j))));
-            density_term(a, m, h, kn, j, rv, dot(rv, rv), out, stride);
+            f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
+            density_term<kDiv>(a, m, h, kn, j, rv, dot(rv, rv), out, stride, vi, vj);
         }
     } else {
         walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
-            density_term(a, m, h, kn, j, rv, r2, out, stride);
+            if (kDiv) vj = __ldg(kDiv == 1 ? velb(B, j) : vela(B, j));
+            density_term<kDiv>(a, m, h, kn, j, rv, r2, out, stride, vi, vj);
         });
     }
+    if (kDiv) B.src[i] = -a.div;   // divergence_source_term.comp:58-60
     B.rho[i] = a.density;
     // velocity_b.w carries the density for the neighbour gathers of viscosity
     // and the FIXED-mode divergence source
@@ -381,8 +408,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_density_alph
     __shared__ DensityScratch scratch[kThreads / 32];
     DensityScratch& S = scratch[threadIdx.x >> 5];
     for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-        density_alpha_particle(B, S, i, s, live);
+        density_alpha_particle<0>(B, S, i, s, live);
     });
+}
+
+// density_alpha with the (plain) divergence source of the same substep
+// summed in its pair loop: the divergence source needs exactly these pairs,
+// gradients and order, and the neighbour's velocity shares a 32-byte record
+// with the position copy the loop loads.  fixed: FIXED mode (velocity_b),
+// else REFERENCE mode (velocity_a).
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
+    k_density_alpha_div(Bufs B, int fixed) {
+    __shared__ DensityScratch scratch[kThreads / 32];
+    DensityScratch& S = scratch[threadIdx.x >> 5];
+    if (fixed) {
+        for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+            density_alpha_particle<1>(B, S, i, s, live);
+        });
+    } else {
+        for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+            density_alpha_particle<2>(B, S, i, s, live);
+        });
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1041,5 +1089,9 @@ template __global__ void k_density_alpha<128, false>(Bufs);
 template __global__ void k_density_alpha<256, false>(Bufs);
 template __global__ void k_density_alpha<128, true>(Bufs);
 template __global__ void k_density_alpha<256, true>(Bufs);
+template __global__ void k_density_alpha_div<128, false>(Bufs, int);
+template __global__ void k_density_alpha_div<256, false>(Bufs, int);
+template __global__ void k_density_alpha_div<128, true>(Bufs, int);
+template __global__ void k_density_alpha_div<256, true>(Bufs, int);
 
 }  // namespace fe

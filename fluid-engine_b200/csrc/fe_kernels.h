@@ -25,6 +25,8 @@ __global__ void k_refresh_pr(Bufs B);
 template <int kThreads, bool kPersist>
 __global__ void k_density_alpha(Bufs B);
 template <int kThreads, bool kPersist>
+__global__ void k_density_alpha_div(Bufs B, int fixed);
+template <int kThreads, bool kPersist>
 __global__ void k_viscosity(Bufs B);
 // Per-scene finishes of a multi-scene context, one block per scene.
 __global__ void k_solve_finish(Bufs B, int which, cudaGraphConditionalHandle handle,

@@ -88,13 +88,17 @@ class TrainResult:
 
 
 def capture(workload_names=("dam_break_16k", "dam_break_256k"), frames=(100, 300),
-            strides=(32, 1536), capacity=120_000, warmup=2, device=0, seed=1):
-    """Runs the plain tolerance solver and returns captured (x[n][12], y[n][2]).
+            strides=(32, 1536), capacity=120_000, warmup=2, device=0, seed=1, model=None):
+    """Runs the tolerance solver and returns captured (x[n][12], y[n][2]).
 
     The defaults sample the 16,384-particle dam break (fixed dt 1 ms) over 100
     frames and the 262,144-particle one (adaptive CFL) over 300 frames, about
     100k solve snapshots each: a sample is taken for a (particle, substep,
-    solve) triple whose hash is 0 modulo the stride."""
+    solve) triple whose hash is 0 modulo the stride.  Without `model` the
+    plain solver runs; with it, the solves start from that network's warm
+    start (the features then carry the pressures of learned-started solves,
+    and the divergence target is relative to the density solve's pressure as
+    the warm start sees it)."""
     lib = load_library()
     xs, ys = [], []
     for name, nf, stride in zip(workload_names, frames, strides):
@@ -102,9 +106,13 @@ def capture(workload_names=("dam_break_16k", "dam_break_256k"), frames=(100, 300
         p = _abi.copy_params(w.params)
         p.solver = _abi.FE_SOLVER_TOLERANCE
         p.mode = _abi.FE_MODE_FIXED
+        if model is not None:
+            p.warm_start = _abi.FE_WARM_LEARNED
         w.seed = seed
         sim = Simulation(w.positions(), p, device=device)
         h = sim.data.handle
+        if model is not None:
+            check(lib, lib.fe_set_model(h, model.handle), "fe_set_model")
         for _ in range(warmup):
             sim.step(1)
         check(lib, lib.fe_capture_begin(h, capacity, stride), "fe_capture_begin")
@@ -174,6 +182,23 @@ def train(x: np.ndarray, y: np.ndarray, *, epochs: int = 30, batch: int = 4096,
             log(f"epoch {ep}: loss {losses[-1]:.4f}")
     val = evaluate(model, xv, yv)
     return TrainResult(model, losses, val, int(x.shape[0]))
+
+
+def train_on_own_starts(epochs: int = 30, device: int = 0, log=None) -> TrainResult:
+    """Two rounds of capture and training.  The first network learns from the
+    plain solver.  Its divergence output, though, corrects the density
+    solve's pressure, and under the warm start that pressure comes from a
+    learned-started density solve, not a plain one.  So the same scenes are
+    captured again with the first network's warm start, and the final
+    network is trained on both captures (the capture order is canonical, so
+    the result is repeatable)."""
+    x1, y1 = capture(device=device)
+    first = train(x1, y1, epochs=epochs, device=device, log=log)
+    x2, y2 = capture(device=device, model=first.model)
+    first.model.close()
+    x = np.concatenate([x1, x2])
+    y = np.concatenate([y1, y2])
+    return train(x, y, epochs=epochs, device=device, log=log)
 
 
 def predict(model: Model, x: np.ndarray) -> np.ndarray:
