@@ -481,11 +481,22 @@ fe_status rec_density_alpha(fe_ctx* c, Recorder& R) {
                    c->B);
 }
 
-// density_alpha that also sums the plain divergence source (the mid-substep
-// neighbour search's pass, when no learned state rides along).
+// density_alpha that also sums the divergence source (the mid-substep
+// neighbour search's pass); with the learned state it also emits the
+// divergence solve's features.
 fe_status rec_density_alpha_div(fe_ctx* c, Recorder& R) {
     const int g = FE_NBR_DENSITY_ALPHA;
     const uint32_t t = c->nbr_threads[g];
+    if (c->carries())
+        return rec_nbr(c, R, g,
+                       c->nbr_persistent[g]
+                           ? pick(k_density_alpha_div_learn<128, true>,
+                                  k_density_alpha_div_learn<256, true>,
+                                  k_density_alpha_div_learn<256, true>, t)
+                           : pick(k_density_alpha_div_learn<128, false>,
+                                  k_density_alpha_div_learn<256, false>,
+                                  k_density_alpha_div_learn<256, false>, t),
+                       c->B, c->fixed_mode() ? 1 : 0, c->L);
     return rec_nbr(c, R, g,
                    c->nbr_persistent[g]
                        ? pick(k_density_alpha_div<128, true>, k_density_alpha_div<256, true>,
@@ -524,12 +535,6 @@ fe_status rec_list_pass(fe_ctx* c, Recorder& R, int pass) {
                 return rec_nbr(c, R, g, NBR_KERNEL(k_density_source_learn, g), c->B, c->L);
             return rec_nbr(c, R, g, NBR_KERNEL(k_density_source, g), c->B);
         default:
-            if (c->carries() && fixed)
-                return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source_learn_fixed, g), c->B,
-                               c->L);
-            if (c->carries())
-                return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source_learn, g), c->B, fixed,
-                               c->L);
             return rec_nbr(c, R, g, NBR_KERNEL(k_divergence_source, g), c->B, fixed);
     }
 }
@@ -682,12 +687,7 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
     else if ((s = rec_simple(c, R, k_pressure_integration)))
         return s;
     if ((s = rec_neighbor_search(c, R))) return s;
-    if (c->carries()) {   // the learned source needs this pass's densities
-        if ((s = rec_density_alpha(c, R))) return s;
-        if ((s = rec_list_pass(c, R, 2))) return s;
-    } else if ((s = rec_density_alpha_div(c, R))) {
-        return s;
-    }
+    if ((s = rec_density_alpha_div(c, R))) return s;
     if (c->learned()) {   // ... and the divergence solve
         if ((s = rec_mlp(c, R, 1))) return s;
         if ((s = rec_trace(c, R, 2 * k + 1))) return s;
@@ -1724,11 +1724,13 @@ static fe_status ensure_learn_buffers(fe_ctx* c) {
     fe_status s;
     __nv_bfloat16* xb = nullptr;
     if ((s = dev_alloc(c, &xb, (size_t)c->n * 16)) || (s = dev_alloc(c, &c->L.out, 2 * (size_t)c->n)) ||
-        (s = dev_alloc(c, &c->L.carry_tmp, c->n)))
+        (s = dev_alloc(c, &c->L.carry_tmp, c->n)) || (s = dev_alloc(c, &c->L.mom, c->n)) ||
+        (s = dev_alloc(c, &c->L.mom_tmp, c->n)))
         return s;
     float4* carry = nullptr;
     if ((s = dev_alloc(c, &carry, c->n))) return s;
     c->L.xb = xb;
+    FE_CUDA(cudaMemsetAsync(c->L.mom, 0, (size_t)c->n * 16, c->stream));
     FE_CUDA(cudaMemsetAsync(carry, 0, (size_t)c->n * 16, c->stream));
     // no capture slot yet: w = all ones
     FE_CUDA(cudaMemset2DAsync(reinterpret_cast<char*>(carry) + 12, 16, 0xFF, 4, c->n, c->stream));

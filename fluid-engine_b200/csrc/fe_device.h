@@ -120,14 +120,19 @@ struct Bufs {
 // Learned warm start and training-data capture (fe_learned.cu).
 // carry[i] travels with particle i through every re-sort:
 //   x = final pressure of the last density solve, y = of the last
-//   divergence solve, z unused, w = capture slot of the solve in progress
-//   (bits; ~0 none).
+//   divergence solve, z = the fifth neighbourhood moment of the substep
+//   (feature 11), w = capture slot of the solve in progress (bits; ~0 none).
+// mom[i] = features 7..10 (the first four moments), with z above the
+// moments the density source computed at the substep's start; the
+// divergence solve's features reuse them after the mid-substep re-sort.
 struct LearnArgs {
     const float* norm;          // model standardisation: x mean[12], std[12], y mean[2], std[2]
     void* xb;                   // BF16 feature rows [n][16] (network input)
     float* out;                 // network output [n][2] (standardised)
     float4* carry;
     float4* carry_tmp;
+    float4* mom;
+    float4* mom_tmp;
     float* cap_x;               // captured raw features [capacity][12]
     float* cap_y;               // captured normalised targets [capacity][2]
     uint32_t* cap_count;

@@ -19,7 +19,11 @@
 //   7..11  the 5 lowest moments (orders 1..5) of the neighbours' density
 //          residual, t_j = x / (1 + |x|) with x = 100 (rho_j / rho0 - 1),
 //          weighted by -grad_factor / (h r) (the list's kernel-gradient
-//          scale, >= 0): sum_j w_j t_j^k / sum_j w_j
+//          scale, >= 0): sum_j w_j t_j^k / sum_j w_j, as the density source
+//          finds them at the start of the substep.  The divergence solve's
+//          row carries the same five values through the mid-substep re-sort
+//          (LearnArgs::mom, carry.z), so its features need no neighbour pass
+//          of their own and are emitted by density_alpha.
 // ("last" = the most recent solve of that kind: before the divergence solve
 // the density kappa is the one just computed in this substep.)  The solve's
 // own source term in the same units is a fixed linear combination of
@@ -83,12 +87,20 @@ struct Moments {
     }
 };
 
+// The five moment features from the running sums.
+__device__ __forceinline__ void moment_features(const Moments& mo, float fm[kMoments]) {
+#pragma unroll
+    for (int k = 0; k < kMoments; ++k) fm[k] = mo.w > 0.0f ? mo.m[k] / mo.w : 0.0f;
+}
+
 // Writes the network input row (learned mode) and captures a sample
-// (capture mode) for particle i before solve `which` (0 density, 1 divergence).
+// (capture mode) for particle i before solve `which` (0 density, 1
+// divergence); fm = its five moment features.  Before the density solve the
+// moments are also stored for the divergence solve (mom, carry.z).
 __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
                                               const DevParams& P, uint32_t i, uint32_t scene,
                                               int which, float div_i, f3 v,
-                                              const Moments& mo) {
+                                              const float fm[kMoments]) {
     const float h = P.h, m = P.mass, dt = P.dt, rho0 = P.rho0;
     const float rho = B.rho[i], alpha = B.alpha[i];
     const float scale = kappa_scale(rho, alpha, dt, rho0);
@@ -104,7 +116,8 @@ __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
     f[5] = scale > 0.0f ? carry.y / scale : 0.0f;
     f[6] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * dt / h;
 #pragma unroll
-    for (int k = 0; k < kMoments; ++k) f[7 + k] = mo.w > 0.0f ? mo.m[k] / mo.w : 0.0f;
+    for (int k = 0; k < kMoments; ++k) f[7 + k] = fm[k];
+    if (which == 0) L.mom[i] = make_float4(fm[0], fm[1], fm[2], fm[3]);
 
     if (L.learned) {
         uint32_t packed[8];
@@ -133,7 +146,10 @@ __device__ __forceinline__ void emit_features(const Bufs& B, const LearnArgs& L,
             L.cap_y[2 * (size_t)k + 1] = nan;  // the other stays NaN (not trained)
         }
     }
-    L.carry[i].w = __uint_as_float(slot);
+    // z: the fifth moment for the divergence solve (kept by that solve's
+    // emission), w: the capture slot
+    float2* zw = reinterpret_cast<float2*>(&L.carry[i]) + 1;
+    *zw = make_float2(which == 0 ? fm[4] : carry.z, __uint_as_float(slot));
 }
 
 // Applies the network's pressure to the solve about to start (output

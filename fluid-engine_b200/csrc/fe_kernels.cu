@@ -90,7 +90,10 @@ __device__ __forceinline__ void reorder_body(const Bufs& B, int carry_pressure,
     st_pair(B.pv, i, p, *vela(B, src));
     st_pair(B.pa, i, p, *vela(B, i));
     if (carry_pressure) B.prs_tmp[i] = B.prs[src];
-    if (kCarry) L.carry_tmp[i] = L.carry[src];
+    if (kCarry) {
+        L.carry_tmp[i] = L.carry[src];
+        L.mom_tmp[i] = L.mom[src];
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) k_reorder(Bufs B, int carry_pressure) {
@@ -111,7 +114,10 @@ __device__ __forceinline__ void take_pressure_body(const Bufs& B, const LearnArg
     float p = B.prs_tmp[i];
     B.prs[i] = p;
     posb(B, i)->w = pressure_over_rho2(p, B.rho[i]);
-    if (kCarry) L.carry[i] = L.carry_tmp[i];
+    if (kCarry) {
+        L.carry[i] = L.carry_tmp[i];
+        L.mom[i] = L.mom_tmp[i];
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) k_take_pressure(Bufs B) {
@@ -323,9 +329,13 @@ constexpr int kMinBlocks = 1024 / kThreads;
 // kDiv: 0 density and alpha only; 1 also the FIXED-mode divergence source
 // (velocity_b), 2 also the REFERENCE-mode one (velocity_a) -- see
 // density_term.
-template <int kDiv>
+// kLearn (with kDiv): also the divergence solve's feature row, from this
+// pass's density, factor, count and source and the moments carried from
+// the substep's density source.
+template <int kDiv, bool kLearn>
 __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScratch& S,
-                                                       uint32_t i, uint32_t s, bool live) {
+                                                       uint32_t i, uint32_t s, bool live,
+                                                       const LearnArgs& L) {
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
     const float kn = kernel_norm(h);
@@ -401,6 +411,11 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     B.nbr_count[i] = a.cnt;
     posb(B, i)->w = pressure_over_rho2(B.prs[i], a.density);
     if (a.cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
+    if (kLearn) {
+        const float4 m4 = L.mom[i];
+        const float fm[kMoments] = {m4.x, m4.y, m4.z, m4.w, L.carry[i].z};
+        emit_features(B, L, P, i, s, 1, a.div, vi, fm);
+    }
 }
 
 template <int kThreads, bool kPersist>
@@ -408,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_density_alph
     __shared__ DensityScratch scratch[kThreads / 32];
     DensityScratch& S = scratch[threadIdx.x >> 5];
     for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-        density_alpha_particle<0>(B, S, i, s, live);
+        density_alpha_particle<0, false>(B, S, i, s, live, LearnArgs{});
     });
 }
 
@@ -424,11 +439,28 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
     DensityScratch& S = scratch[threadIdx.x >> 5];
     if (fixed) {
         for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-            density_alpha_particle<1>(B, S, i, s, live);
+            density_alpha_particle<1, false>(B, S, i, s, live, LearnArgs{});
         });
     } else {
         for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-            density_alpha_particle<2>(B, S, i, s, live);
+            density_alpha_particle<2, false>(B, S, i, s, live, LearnArgs{});
+        });
+    }
+}
+
+// The same with the learned state: also the divergence solve's features.
+template <int kThreads, bool kPersist>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
+    k_density_alpha_div_learn(Bufs B, int fixed, LearnArgs L) {
+    __shared__ DensityScratch scratch[kThreads / 32];
+    DensityScratch& S = scratch[threadIdx.x >> 5];
+    if (fixed) {
+        for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+            density_alpha_particle<1, true>(B, S, i, s, live, L);
+        });
+    } else {
+        for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
+            density_alpha_particle<2, true>(B, S, i, s, live, L);
         });
     }
 }
@@ -499,7 +531,11 @@ __device__ __forceinline__ void density_source_body(const Bufs& B, const LearnAr
     B.src[i] = source;
     B.prs[i] = 0.0f;
     posb(B, i)->w = pressure_over_rho2(0.0f, rho_i);
-    if (kLearn) emit_features(B, L, P, i, s, 0, div, vi, mo);
+    if (kLearn) {
+        float fm[kMoments];
+        moment_features(mo, fm);
+        emit_features(B, L, P, i, s, 0, div, vi, fm);
+    }
 }
 
 template <int kThreads, bool kPersist>
@@ -518,61 +554,38 @@ __global__ void __launch_bounds__(kThreads, (3 * kMinBlocks<kThreads>) / 4)
 
 // ---------------------------------------------------------------------------
 // divergence_source_term.comp:14-61 (velocities = velocity_a in REFERENCE
-// mode, velocity_b in FIXED mode); kLearn as above.
+// mode, velocity_b in FIXED mode).
 // ---------------------------------------------------------------------------
-template <bool kLearn>
-__device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed,
-                                                       const LearnArgs& L, uint32_t i,
+__device__ __forceinline__ void divergence_source_body(const Bufs& B, int fixed, uint32_t i,
                                                        uint32_t s) {
     const DevParams& P = B.P[s];
     const float m = P.mass;
     const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(fixed ? velb(B, i) : vela(B, i)));
     float div = 0.0f;
-    Moments mo;
-    auto term = [&](f3 rv, float g, float4 vj, float rho_j) {
+    auto term = [&](f3 rv, float g, float4 vj) {
         f3 grad = scale(g, rv);
         f3 vd = sub(vi, xyz(vj));
         div += m * dot(vd, grad);
-        if (kLearn) mo.add(g, rho_j, P.rho0);
     };
     if (fixed) {
-        // velocity_b and its density from the position/velocity record
-        for_each_neighbor_pair(B, P, i, pi, B.pv,
-                               [&](f3 rv, float g, float4 vj) { term(rv, g, vj, vj.w); });
+        // velocity_b from the position/velocity record
+        for_each_neighbor_pair(B, P, i, pi, B.pv, [&](f3 rv, float g, float4 vj) { term(rv, g, vj); });
     } else {
         for_each_neighbor(
-            B, P, i, pi,
-            [&](uint32_t j) {
-                return VelRho{__ldg(vela(B, j)), kLearn ? __ldg(B.rho + j) : 0.0f};
-            },
-            [&](uint32_t, f3 rv, float g, float4, VelRho d) { term(rv, g, d.v, d.rho); });
+            B, P, i, pi, [&](uint32_t j) { return __ldg(vela(B, j)); },
+            [&](uint32_t, f3 rv, float g, float4, float4 vj) { term(rv, g, vj); });
     }
     B.src[i] = -div;
-    if (kLearn) emit_features(B, L, P, i, s, 1, div, vi, mo);
 }
 
+// The stand-alone pass (the stage call; a frame sums it inside
+// density_alpha, k_density_alpha_div).
 template <int kThreads, bool kPersist>
 __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_divergence_source(Bufs B,
                                                                                       int fixed) {
     for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-        if (live) divergence_source_body<false>(B, fixed, LearnArgs{}, i, s);
-    });
-}
-// FIXED mode with the learned state: the mode is a constant, so only the
-// record path is compiled (fewer registers, four blocks of 256 per SM).
-template <int kThreads, bool kPersist>
-__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
-    k_divergence_source_learn_fixed(Bufs B, LearnArgs L) {
-    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-        if (live) divergence_source_body<true>(B, 1, L, i, s);
-    });
-}
-template <int kThreads, bool kPersist>
-__global__ void __launch_bounds__(kThreads, (3 * kMinBlocks<kThreads>) / 4)
-    k_divergence_source_learn(Bufs B, int fixed, LearnArgs L) {
-    for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
-        if (live) divergence_source_body<true>(B, fixed, L, i, s);
+        if (live) divergence_source_body(B, fixed, i, s);
     });
 }
 
@@ -1076,8 +1089,6 @@ __global__ void k_count_substep(Bufs B) {
     template __global__ void k_density_source<T, P>(Bufs);                            \
     template __global__ void k_density_source_learn<T, P>(Bufs, LearnArgs);           \
     template __global__ void k_divergence_source<T, P>(Bufs, int);                    \
-    template __global__ void k_divergence_source_learn<T, P>(Bufs, int, LearnArgs);   \
-    template __global__ void k_divergence_source_learn_fixed<T, P>(Bufs, LearnArgs);  \
     template __global__ void k_pressure_force<T, P>(Bufs, int);
 FE_NBR_INSTANTIATE(128, false)
 FE_NBR_INSTANTIATE(256, false)
@@ -1093,5 +1104,9 @@ template __global__ void k_density_alpha_div<128, false>(Bufs, int);
 template __global__ void k_density_alpha_div<256, false>(Bufs, int);
 template __global__ void k_density_alpha_div<128, true>(Bufs, int);
 template __global__ void k_density_alpha_div<256, true>(Bufs, int);
+template __global__ void k_density_alpha_div_learn<128, false>(Bufs, int, LearnArgs);
+template __global__ void k_density_alpha_div_learn<256, false>(Bufs, int, LearnArgs);
+template __global__ void k_density_alpha_div_learn<128, true>(Bufs, int, LearnArgs);
+template __global__ void k_density_alpha_div_learn<256, true>(Bufs, int, LearnArgs);
 
 }  // namespace fe

@@ -27,6 +27,8 @@ __global__ void k_density_alpha(Bufs B);
 template <int kThreads, bool kPersist>
 __global__ void k_density_alpha_div(Bufs B, int fixed);
 template <int kThreads, bool kPersist>
+__global__ void k_density_alpha_div_learn(Bufs B, int fixed, LearnArgs L);
+template <int kThreads, bool kPersist>
 __global__ void k_viscosity(Bufs B);
 // Per-scene finishes of a multi-scene context, one block per scene.
 __global__ void k_solve_finish(Bufs B, int which, cudaGraphConditionalHandle handle,
@@ -53,10 +55,6 @@ __global__ void k_frame_prologue(Bufs B);
 __global__ void k_count_substep(Bufs B);
 template <int kThreads, bool kPersist>
 __global__ void k_density_source_learn(Bufs B, LearnArgs L);
-template <int kThreads, bool kPersist>
-__global__ void k_divergence_source_learn(Bufs B, int fixed, LearnArgs L);
-template <int kThreads, bool kPersist>
-__global__ void k_divergence_source_learn_fixed(Bufs B, LearnArgs L);
 __global__ void k_carry_take(Bufs B, LearnArgs L);
 __global__ void k_stats_snapshot(Bufs B, StatsSnapshot* dst, uint32_t scene);
 __global__ void k_snapshot4(float4* dst, const float4* src, uint32_t stride, uint32_t n,

@@ -14,6 +14,7 @@
 #include "fe_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -385,6 +386,9 @@ struct State : Base {
     // particle from the last density_alpha (duplicates of a doubly visited
     // bucket counted twice, like the walk)
     std::vector<V4<R>> carry, carry_tmp;
+    // the five moment features of the substep's density source, carried
+    // through the mid-substep re-sort for the divergence solve's row
+    std::vector<std::array<R, 5>> mom, mom_tmp;
     std::vector<uint32_t> nbr_count;
 
     R h() const { return (R)p.smoothing_radius; }
@@ -468,10 +472,16 @@ struct State : Base {
             pos_b[i] = pos_a[s];
             vel_b[i] = vel_a[s];
             if (fixed) prs_tmp[i] = prs[s];
-            if (learned) carry_tmp[i] = carry[s];
+            if (learned) {
+                carry_tmp[i] = carry[s];
+                mom_tmp[i] = mom[s];
+            }
         }
         if (fixed) std::swap(prs, prs_tmp);
-        if (learned) std::swap(carry, carry_tmp);
+        if (learned) {
+            std::swap(carry, carry_tmp);
+            std::swap(mom, mom_tmp);
+        }
         return 0;
     }
 
@@ -551,7 +561,10 @@ struct State : Base {
             if (d > K<R>::eps_r()) source = ((rho0 - rho[i]) / d) - div;
             src[i] = source;
             prs[i] = 0;
-            if (learned) emit_row(i, 0, div, vi, mo);
+            if (learned) {
+                for (int k = 0; k < 5; ++k) mom[i][k] = mo.w > R(0) ? mo.m[k] / mo.w : R(0);
+                emit_row(i, 0, div, vi, mom[i].data());
+            }
         }
     }
 
@@ -583,8 +596,9 @@ struct State : Base {
 
     // emit_features (fe_features.cuh): the 12 features of particle i before
     // solve `which`, standardised with the model's statistics, as the BF16
-    // row the network reads.
-    void emit_row(uint32_t i, int which, R div, V3<R> v, const Moments& mo) {
+    // row the network reads; fm = its five moment features (the density
+    // source's, carried for the divergence solve).
+    void emit_row(uint32_t i, int which, R div, V3<R> v, const R* fm) {
         uint32_t slot = 2u * cur_substep + (uint32_t)which;
         if (slot >= net_slots) return;
         R hh = h(), m = mass(), d = dt(), rho0 = (R)p.target_density;
@@ -600,7 +614,7 @@ struct State : Base {
         f[4] = sc > R(0) ? carry[i].x / sc : R(0);
         f[5] = sc > R(0) ? carry[i].y / sc : R(0);
         f[6] = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z) * d / hh;
-        for (int k = 0; k < 5; ++k) f[7 + k] = mo.w > R(0) ? mo.m[k] / mo.w : R(0);
+        for (int k = 0; k < 5; ++k) f[7 + k] = fm[k];
         uint16_t* row = rows.data() + ((size_t)slot * n + i) * 16;
         for (int k = 0; k < 16; ++k) {
             R a = k < 12 ? (f[k] - (R)norm[k]) / (R)norm[12 + k] : R(0);
@@ -658,26 +672,23 @@ struct State : Base {
     // divergence_source_term.comp:14-61 (velocities = velocity_a in
     // REFERENCE mode, divergence_source_term.rs:47).
     void divergence_source() override {
-        R m = mass(), hh = h(), rho0 = (R)p.target_density;
+        R m = mass(), hh = h();
         const std::vector<V4<R>>& vel = vel_div();
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads())
         for (long long ii = 0; ii < (long long)n; ++ii) {
             uint32_t i = (uint32_t)ii;
             V3<R> vi = xyz(vel[i]);
             R div = 0;
-            Moments mo;
             for_neighbors(i, [&](uint32_t j, V3<R> rv, R r2) {
                 R r = std::sqrt(r2);
                 if (r > K<R>::eps_r()) {
-                    R g = kernel_grad_scale(r, hh);
-                    V3<R> grad = scale(g, rv);
+                    V3<R> grad = scale(kernel_grad_scale(r, hh), rv);
                     V3<R> vd = sub(vi, xyz(vel[j]));
                     div += m * dot(vd, grad);
-                    if (learned) mo.add(g, rho[j], rho0);
                 }
             });
             src[i] = -div;
-            if (learned) emit_row(i, 1, div, vi, mo);
+            if (learned) emit_row(i, 1, div, vi, mom[i].data());
         }
     }
 
@@ -917,6 +928,8 @@ Base* make_state(const fe_params* params, uint32_t n, const float* pos, const fl
     s->prs.assign(n, 0);
     s->prs_tmp.assign(n, 0);
     s->carry.assign(n, {0, 0, 0, 0});
+    s->mom.assign(n, {0, 0, 0, 0, 0});
+    s->mom_tmp.assign(n, {0, 0, 0, 0, 0});
     s->carry_tmp.assign(n, {0, 0, 0, 0});
     s->nbr_count.assign(n, 0);
     s->ekey.assign(s->T, 0);
