@@ -229,10 +229,10 @@ def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = Fal
     # offsets, reorder (+ pressure carry in FIXED mode, + learned state)
     ns = 1 + 1 + 1 + passes + 1 + 1 + 1 + (1 if fixed_mode else 0) + \
         (1 if learned and not fixed_mode else 0)
-    # viscosity, density source, 2 x (solve begin + end), integration, density/alpha,
-    # divergence source (plain: summed inside density/alpha), divergence
+    # viscosity, density source, 2 x (solve begin + end), integration,
+    # density/alpha (with the divergence source summed in), divergence
     # integration, substep counter
-    fixed = 1 + 1 + 4 + 1 + 1 + (1 if learned else 0) + 1 + 1
+    fixed = 1 + 1 + 4 + 1 + 1 + 1 + 1
     # per Jacobi iteration: force, update, loop guard
     iters = 3 * (stats.density_iterations + stats.divergence_iterations)
     # learned: 2 x the network (which also applies the start); features,
