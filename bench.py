@@ -85,6 +85,7 @@ class ClockSampler:
         self.proc = None
         self.thread = None
         self.stop = threading.Event()
+        self.ready = threading.Event()   # set once the poller has taken a sample
 
     def _nvml_handle(self):
         import pynvml
@@ -110,6 +111,7 @@ class ClockSampler:
                                      [n for n, b in bits.items() if r & b]))
             except Exception:
                 pass
+            self.ready.set()
             self.stop.wait(self.period)
 
     def _poll_smi(self):
@@ -125,6 +127,8 @@ class ClockSampler:
                                       if v.lower().startswith("active")]))
             except (ValueError, IndexError):
                 continue
+            finally:
+                self.ready.set()
 
     def __enter__(self):
         try:
@@ -143,6 +147,11 @@ class ClockSampler:
                 self.thread = None
         if self.thread:
             self.thread.start()
+            # the poller is running before the timed region starts, so its
+            # 10 ms samples fall inside even a short region; the sample taken
+            # before the region is dropped
+            self.ready.wait(timeout=2.0)
+            self.skip = len(self.samples)
         return self
 
     def __exit__(self, *a):
@@ -157,12 +166,16 @@ class ClockSampler:
             self.thread.join(timeout=5)
 
     def summary(self):
-        if not self.samples:
+        # the samples taken inside the region; only when there are none (a
+        # region shorter than the period), the one taken just before it
+        inside = self.samples[getattr(self, "skip", 0):]
+        samples = inside or self.samples
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        reasons = sorted({n for _, _, rs in self.samples for n in rs})
-        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
-                "sm_max_mhz": self.samples[-1][1], "reasons": reasons,
-                "samples": len(self.samples),
+        reasons = sorted({n for _, _, rs in samples for n in rs})
+        return {"sm_mhz": statistics.median(s[0] for s in samples),
+                "sm_max_mhz": samples[-1][1], "reasons": reasons,
+                "samples": len(samples), "during_region": bool(inside),
                 "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 

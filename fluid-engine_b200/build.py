@@ -6,6 +6,12 @@ Device code is compiled with -fmad=false -prec-div=true -prec-sqrt=true
 -ftz=false: every float operation rounds once, in source order, so the
 kernels reproduce the host oracle bit for bit.  The library links the CUDA
 runtime statically and exports only the C ABI of include/fluid_step.h.
+
+A second library, libfluidstep_contract.so, is the same C ABI with the
+physics kernels (fe_kernels.cu) compiled with -fmad=true: the compiler may
+contract a multiply and an add into one fused multiply-add.  Its results
+are checked against the FP64 evaluation of the step within a relative
+tolerance instead of bit for bit.
 """
 from __future__ import annotations
 
@@ -17,6 +23,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "fluid_step", "libfluidstep.so")
+CONTRACT_OUT = os.path.join(HERE, "fluid_step", "libfluidstep_contract.so")
+CONTRACT_SOURCES = ["fe_kernels.cu"]
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = ["fe_kernels.cu", "fe_sort.cu", "fe_api.cu", "fe_sort_noalloc.cu", "fe_mlp.cu", "fe_tune.cu",
@@ -62,13 +70,37 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 f.write(log)
             if verbose:
                 sys.stdout.write(log)
-    if force or newer(OUT, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs + ["-Xcompiler", "-fPIC"]
+    link(OUT, objs, force)
+    # the contraction build: the physics kernels again with -fmad=true
+    contract_flags = ["-fmad=true" if f == "-fmad=false" else f for f in FLAGS]
+    cobjs = []
+    for o, src in zip(objs, SOURCES):
+        if src not in CONTRACT_SOURCES:
+            cobjs.append(o)
+            continue
+        s = os.path.join(CSRC, src)
+        co = os.path.join(BUILD, src.replace(".cu", "_contract.o"))
+        cobjs.append(co)
+        if force or newer(co, [s] + headers):
+            cmd = [nvcc()] + ARCH + contract_flags + ["-c", s, "-o", co]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            log = r.stdout + r.stderr
+            if r.returncode != 0:
+                sys.stderr.write(log)
+                raise RuntimeError(f"nvcc failed on {src} (contraction build)")
+            with open(co + ".log", "w") as f:
+                f.write(log)
+    link(CONTRACT_OUT, cobjs, force)
+    return OUT
+
+
+def link(out: str, objs, force: bool) -> None:
+    if force or newer(out, objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", out] + objs + ["-Xcompiler", "-fPIC"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError("link failed")
-    return OUT
+            raise RuntimeError(f"link of {os.path.basename(out)} failed")
 
 
 if __name__ == "__main__":

@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_density_sour
     });
 }
 template <int kThreads, bool kPersist>
-__global__ void __launch_bounds__(kThreads, (3 * kMinBlocks<kThreads>) / 4)
+__global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
     k_density_source_learn(Bufs B, LearnArgs L) {
     for_each_particle<kThreads, kPersist>(B, [&](uint32_t i, uint32_t s, bool live) {
         if (live) density_source_body<true>(B, L, i, s);

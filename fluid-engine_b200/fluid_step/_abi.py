@@ -270,21 +270,33 @@ def copy_params(p: FeParams) -> FeParams:
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PACKAGE_DIR, "libfluidstep.so")
+# The same C ABI with the physics kernels compiled with fused multiply-add
+# contraction: within a relative tolerance of the FP64 step, not bit-exact.
+CONTRACT_LIB_PATH = os.path.join(PACKAGE_DIR, "libfluidstep_contract.so")
+BUILDS = {"parity": LIB_PATH, "contract": CONTRACT_LIB_PATH}
 
 _lib = None
+_libs: dict = {}
 
 
 class LibraryMissing(RuntimeError):
     pass
 
 
-def load_library(path: str | None = None):
-    """Loads libfluidstep.so from the package directory.
+def load_library(path: str | None = None, *, build: str = "parity"):
+    """Loads libfluidstep.so from the package directory (build="contract":
+    libfluidstep_contract.so, the fused multiply-add build).
 
     Raises LibraryMissing when the library was not built: there is no other
     implementation to fall back to.
     """
     global _lib
+    if path is None and build != "parity":
+        if build not in BUILDS:
+            raise ValueError(f"unknown build {build!r} (expected one of {sorted(BUILDS)})")
+        if build not in _libs:
+            _libs[build] = load_library(BUILDS[build])
+        return _libs[build]
     if _lib is not None and path is None:
         return _lib
     path = path or LIB_PATH

@@ -33,8 +33,8 @@ class GpuPhysicsData:
     particles and a hash table of next_pow2(N) entries."""
 
     def __init__(self, initial_positions, sim_params: _abi.FeParams, *, velocities=None,
-                 device: int = 0):
-        self._lib = load_library()
+                 device: int = 0, build: str = "parity"):
+        self._lib = load_library(build=build)
         pos = np.ascontiguousarray(initial_positions, dtype=np.float32).reshape(-1, 3)
         vel = None if velocities is None else np.ascontiguousarray(
             velocities, dtype=np.float32).reshape(-1, 3)
@@ -321,9 +321,10 @@ class ComputePipelines:
 class Simulation:
     """The whole frame through fe_step (graph-replayed on the device)."""
 
-    def __init__(self, initial_positions, sim_params, *, velocities=None, device=0):
+    def __init__(self, initial_positions, sim_params, *, velocities=None, device=0,
+                 build="parity"):
         self.data = GpuPhysicsData(initial_positions, sim_params, velocities=velocities,
-                                   device=device)
+                                   device=device, build=build)
         lib = self.data._lib
         check(lib, lib.fe_prepare(self.data.handle), "fe_prepare")
 

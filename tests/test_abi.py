@@ -36,6 +36,16 @@ def test_every_declared_symbol_is_exported(lib):
     assert set(names) == set(_abi.SIGNATURES), set(names) ^ set(_abi.SIGNATURES)
 
 
+def test_contraction_build_exports_the_same_abi(lib):
+    c = _abi.load_library(build="contract")
+    assert c is not lib
+    for n in declared_functions():
+        assert hasattr(c, n), n
+    assert c.fe_abi_version() == _abi.ABI_VERSION
+    with pytest.raises(ValueError):
+        _abi.load_library(build="fast")
+
+
 def test_struct_layout_matches_header(lib):
     fields_p = [f for f, _ in _abi.FeParams._fields_]
     fields_s = [f for f, _ in _abi.FeStats._fields_]
