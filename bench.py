@@ -256,10 +256,11 @@ def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = Fal
 
 
 # ---------------------------------------------------------------------------
-def measure_arm(args, w, params, model, world, local):
+def measure_arm(args, w, params, model, world, local, build="parity"):
     """Warm-up, then K graph-replayed frames timed with CUDA events on the
     context stream, then the same K frames driven through the C ABI with host
-    traffic (e2e), then CUDA-event timing of the hot passes."""
+    traffic (e2e), then CUDA-event timing of the hot passes.  build="contract"
+    runs the fused multiply-add build of the library."""
     import torch
 
     from fluid_step import _abi
@@ -267,7 +268,7 @@ def measure_arm(args, w, params, model, world, local):
 
     pos = w.positions()
     n = pos.shape[0]
-    sim = Simulation(pos, params, device=local)
+    sim = Simulation(pos, params, device=local, build=build)
     lib, h = sim.data._lib, sim.data.handle
     if model is not None:
         _abi.check(lib, lib.fe_set_model(h, model.handle), "fe_set_model")
@@ -692,6 +693,11 @@ def run_gpu(args) -> None:
         arms["learned"] = measure_arm(args, w, lp, model, world, local)
     if args.variant in ("plain", "both"):
         arms["plain"] = measure_arm(args, w, plain_p, None, world, local)
+    # The plain arm once more with the fused multiply-add build of the
+    # physics kernels (within 1e-5 of the FP64 step, not bit-exact).
+    contract = None
+    if args.full_runs:
+        contract = measure_arm(args, w, plain_p, None, world, local, build="contract")
     # Whole runs from rest, both arms: the timed window above covers frames
     # W..W+K only, and the solver's work changes over a run.  The 1M dam break
     # runs its 200 steps at dt = 1 ms; the 262k dam break its 1000 steps with
@@ -814,6 +820,14 @@ def run_gpu(args) -> None:
                                    "kernel_ms": pl["kern"], "clocks": pl["clocks"]}
             out["learned_over_plain"] = head["value"] / pl["value"]
             out["training"] = train_info
+        if contract:
+            out["contraction_build"] = {
+                "arm": "plain Jacobi", "value": contract["value"],
+                "ms_per_step": contract["dev_ms"] / args.steps,
+                "avg_jacobi_iterations": {"density": contract["iters"][0],
+                                          "divergence": contract["iters"][1]},
+                "kernel_ms": contract["kern"], "clocks": contract["clocks"],
+                "library": "libfluidstep_contract.so (-fmad=true physics kernels)"}
         print(json.dumps(out))
     if model is not None:
         model.close()
