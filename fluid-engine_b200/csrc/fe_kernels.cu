@@ -192,6 +192,7 @@ union DensityScratch {
         float4 pos[32];
         uint32_t mask[kMaxSlabs][32];
         RunTable table[kCoopRuns];
+        uint32_t row[kMaxSlabs * 32];   // the run being tested: its candidates' indices
     } coop;
     uint32_t cand[kStage][32];
 };
@@ -249,7 +250,7 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
                                                 uint32_t& n_in) {
     const int lane = lane_id();
     const float h = P.h;
-    const float h2 = h * h;
+    const float h2_wide = (h * h) * (1.0f + 0x1p-18f);
     const uint32_t lt_mask = (1u << lane) - 1u;
     int n_tables = 0;
     while (heads) {
@@ -292,27 +293,24 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
             T.excl[slot] = (uint16_t)excl;
         }
         if (lane == 0) T.excl[__popc(nonempty)] = (uint16_t)total;
+        // the run's row: candidate c of the walk is particle row[c] (each
+        // bucket's lane writes its entries)
+        for (uint32_t u = 0; u < len; ++u) S.coop.row[excl + u] = start + u;
+        __syncwarp();
         for (uint32_t sl = 0; sl < nslab; ++sl) {
             const uint32_t cidx = (sl << 5) + (uint32_t)lane;
             const bool valid = cidx < total;
-            // the bucket holding candidate cidx: the last t with excl_t <= cidx
-            int t = 0;
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-                const int probe = t + step;
-                const uint32_t e = __shfl_sync(kFull, excl, probe & 31);
-                if (probe < 27 && e <= cidx) t = probe;
-            }
-            const uint32_t j =
-                __shfl_sync(kFull, start, t) + (cidx - __shfl_sync(kFull, excl, t));
-            const float4 q = valid ? __ldg(posb(B, j)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            // particle p's mask for this slab is the ballot; lane 0 stores it
+            const float4 q =
+                valid ? __ldg(posb(B, S.coop.row[cidx])) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            // particle p's mask for this slab is the ballot; lane 0 stores it.
+            // The test is a superset of the exact r^2 <= h^2 (contracted r^2
+            // against h^2 (1 + 2^-18)); phase 2 applies the exact test.
 #pragma unroll 2
             for (int p = r0; p < r1; ++p) {
                 const float4 a = S.coop.pos[p];
-                const f3 rv = {a.x - q.x, a.y - q.y, a.z - q.z};
-                const float r2 = dot(rv, rv);
-                const uint32_t bits = __ballot_sync(kFull, valid && !(r2 > h2));
+                const float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
+                const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                const uint32_t bits = __ballot_sync(kFull, valid && !(r2 > h2_wide));
                 if (lane == 0) S.coop.mask[sl][p] = bits;
             }
             __syncwarp();
@@ -387,7 +385,9 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
             }
             const uint32_t j = cur_start + (cidx - cur_excl);
             f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
-            density_term<kDiv>(a, m, h, kn, j, rv, dot(rv, rv), out, stride, vi, vj);
+            const float r2 = dot(rv, rv);
+            if (r2 > h * h) continue;   // the shader's test (phase 1 passed a superset)
+            density_term<kDiv>(a, m, h, kn, j, rv, r2, out, stride, vi, vj);
         }
     } else if (!coop && n1 <= (uint32_t)kStage) {
         for (uint32_t k = 0; k < n1; ++k) {
