@@ -305,8 +305,37 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
             // particle p's mask for this slab is the ballot; lane 0 stores it.
             // The test is a superset of the exact r^2 <= h^2 (contracted r^2
             // against h^2 (1 + 2^-18)); phase 2 applies the exact test.
-#pragma unroll 2
-            for (int p = r0; p < r1; ++p) {
+            // two particles of the run per step in packed FP32 (the test
+            // above; the contraction that packing allows is covered by the
+            // widened bound)
+            uint64_t qx2, qy2, qz2;
+            asm("mov.b64 %0, {%1, %1};" : "=l"(qx2) : "f"(q.x));
+            asm("mov.b64 %0, {%1, %1};" : "=l"(qy2) : "f"(q.y));
+            asm("mov.b64 %0, {%1, %1};" : "=l"(qz2) : "f"(q.z));
+            int p = r0;
+#pragma unroll 1
+            for (; p + 1 < r1; p += 2) {
+                const float4 a0 = S.coop.pos[p], a1 = S.coop.pos[p + 1];
+                uint64_t ax, ay, az, dx, dy, dz, r2;
+                asm("mov.b64 %0, {%1, %2};" : "=l"(ax) : "f"(a0.x), "f"(a1.x));
+                asm("mov.b64 %0, {%1, %2};" : "=l"(ay) : "f"(a0.y), "f"(a1.y));
+                asm("mov.b64 %0, {%1, %2};" : "=l"(az) : "f"(a0.z), "f"(a1.z));
+                asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dx) : "l"(ax), "l"(qx2));
+                asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dy) : "l"(ay), "l"(qy2));
+                asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dz) : "l"(az), "l"(qz2));
+                asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(r2) : "l"(dz));
+                asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(r2) : "l"(dy), "l"(r2));
+                asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(r2) : "l"(dx), "l"(r2));
+                float r2a, r2b;
+                asm("mov.b64 {%0, %1}, %2;" : "=f"(r2a), "=f"(r2b) : "l"(r2));
+                const uint32_t b0 = __ballot_sync(kFull, valid && !(r2a > h2_wide));
+                const uint32_t b1 = __ballot_sync(kFull, valid && !(r2b > h2_wide));
+                if (lane == 0) {
+                    S.coop.mask[sl][p] = b0;
+                    S.coop.mask[sl][p + 1] = b1;
+                }
+            }
+            if (p < r1) {
                 const float4 a = S.coop.pos[p];
                 const float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
                 const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
