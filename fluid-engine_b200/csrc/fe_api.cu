@@ -221,6 +221,35 @@ fe_status validate(const fe_params* p) {
     return FE_OK;
 }
 
+// Whether, for the divisor b, the reciprocal step of div_h (fe_common.cuh)
+// returns the correctly rounded r / b for every significand of r: checked
+// over the 2^23 floats of [1, 2), since every step scales exactly with r's
+// exponent.  About 20 ms per new b; the answer is kept per b.
+bool recip_division_exact(float b) {
+    if (!(b > 0.0f) || !std::isfinite(b) || !std::isnormal(b) || !std::isnormal(1.0f / b))
+        return false;
+    static std::mutex mu;
+    static std::vector<std::pair<uint32_t, bool>> known;
+    uint32_t key;
+    std::memcpy(&key, &b, 4);
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& kv : known)
+        if (kv.first == key) return kv.second;
+    const float y = 1.0f / b;
+    bool exact = true;
+    for (uint32_t m = 0; m < (1u << 23) && exact; ++m) {
+        const uint32_t ab = 0x3f800000u | m;
+        float a;
+        std::memcpy(&a, &ab, 4);
+        const float ref = a / b;
+        const float q0 = a * y;
+        const float q = std::fmaf(std::fmaf(-q0, b, a), y, q0);
+        exact = std::memcmp(&ref, &q, 4) == 0;
+    }
+    known.emplace_back(key, exact);
+    return exact;
+}
+
 DevParams to_device(const fe_params& p, uint32_t n, uint32_t T, uint32_t table_base,
                     uint32_t first) {
     DevParams d;
@@ -228,6 +257,8 @@ DevParams to_device(const fe_params& p, uint32_t n, uint32_t T, uint32_t table_b
     d.radius = p.particle_radius;
     d.mass = p.particle_mass;
     d.h = p.smoothing_radius;
+    d.inv_h = 1.0f / p.smoothing_radius;
+    d.h_recip_exact = recip_division_exact(p.smoothing_radius) ? 1u : 0u;
     d.rho0 = p.target_density;
     d.visc = p.viscosity;
     d.omega = p.relax_factor;

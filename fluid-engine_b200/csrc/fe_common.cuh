@@ -83,6 +83,22 @@ __device__ __forceinline__ float kernel_grad_scale_q(float q, float r, float h, 
     return gf / (h * r);
 }
 
+// r / h, correctly rounded.  Where the host has checked, for this h, that
+// the reciprocal step below returns the correctly rounded quotient for every
+// significand of r (h_recip_exact), it is used: q0 = r (1/h) is within an
+// ulp or two, e = r - q0 h is exact in one fused multiply-add, and
+// q0 + e (1/h) rounds to r / h.  The steps scale exactly with r's exponent,
+// so one binade of r covers every normal r (the neighbour loops see r = 0
+// or r of at least about 1e-22, far from underflow).  Otherwise the IEEE
+// division.  Both give the bits of the oracle's r / h.
+__device__ __forceinline__ float div_h(float r, float h, float inv_h, uint32_t exact) {
+    if (exact) {
+        const float q0 = __fmul_rn(r, inv_h);
+        return __fmaf_rn(__fmaf_rn(-q0, h, r), inv_h, q0);
+    }
+    return r / h;
+}
+
 // kernel_w (common.glsl:38-54).
 __device__ __forceinline__ float kernel_w(float r, float h) {
     return kernel_w_q(r / h, kernel_norm(h));

@@ -22,7 +22,8 @@ constexpr uint32_t kNbrCap = 64;     // neighbour-list capacity per particle
 // the frame prologue kernel (adaptive CFL).
 struct DevParams {
     float radius, mass, h, rho0;
-    float visc, omega, dt, pad0;
+    float visc, omega, dt;
+    float inv_h;                        // 1 / h, correctly rounded (div_h)
     float gx, gy, gz, pad1;
     float bminx, bminy, bminz, pad2;
     float bmaxx, bmaxy, bmaxz, pad3;
@@ -34,7 +35,7 @@ struct DevParams {
     uint32_t mode, solver;
     float tol_d, tol_v;
     uint32_t min_it, max_it, warm;
-    uint32_t pad4;
+    uint32_t h_recip_exact;             // div_h may divide by h through inv_h
 };
 
 // Jacobi solve control of one scene (index 0 = density, 1 = divergence).

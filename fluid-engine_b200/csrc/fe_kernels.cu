@@ -208,11 +208,12 @@ struct DensityAcc {
 // sums divergence_source_term.comp's m (v_i - v_j) . grad W over the same
 // pairs in the same order (vi, vj: the velocities that pass binds).
 template <int kDiv>
-__device__ __forceinline__ void density_term(DensityAcc& a, float m, float h, float kn,
+__device__ __forceinline__ void density_term(DensityAcc& a, float m, const DevParams& P, float kn,
                                              uint32_t j, f3 rv, float r2, uint2* out,
                                              uint32_t stride, f3 vi, float4 vj) {
+    const float h = P.h;
     float r = sqrtf(r2);
-    float q = r / h;
+    float q = div_h(r, h, P.inv_h, P.h_recip_exact);
     float w = kernel_w_q(q, kn);
     a.density += m * w;
     if (r > kEpsR) {
@@ -416,18 +417,18 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
             f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
             const float r2 = dot(rv, rv);
             if (r2 > h * h) continue;   // the shader's test (phase 1 passed a superset)
-            density_term<kDiv>(a, m, h, kn, j, rv, r2, out, stride, vi, vj);
+            density_term<kDiv>(a, m, P, kn, j, rv, r2, out, stride, vi, vj);
         }
     } else if (!coop && n1 <= (uint32_t)kStage) {
         for (uint32_t k = 0; k < n1; ++k) {
             uint32_t j = S.cand[k][lane];
             f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
-            density_term<kDiv>(a, m, h, kn, j, rv, dot(rv, rv), out, stride, vi, vj);
+            density_term<kDiv>(a, m, P, kn, j, rv, dot(rv, rv), out, stride, vi, vj);
         }
     } else {
         walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
             if (kDiv) vj = __ldg(kDiv == 1 ? velb(B, j) : vela(B, j));
-            density_term<kDiv>(a, m, h, kn, j, rv, r2, out, stride, vi, vj);
+            density_term<kDiv>(a, m, P, kn, j, rv, r2, out, stride, vi, vj);
         });
     }
     if (kDiv) B.src[i] = -a.div;   // divergence_source_term.comp:58-60
@@ -500,6 +501,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
 __device__ __forceinline__ void viscosity_particle(const Bufs& B, uint32_t i, uint32_t s) {
     const DevParams& P = B.P[s];
     const float m = P.mass, h = P.h;
+    const float kn = kernel_norm(h), inv_h = P.inv_h;
+    const uint32_t exact = P.h_recip_exact;
     const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(velb(B, i)));
     f3 sum = {0.0f, 0.0f, 0.0f};
@@ -509,7 +512,7 @@ __device__ __forceinline__ void viscosity_particle(const Bufs& B, uint32_t i, ui
         B, P, i, pi, B.pv, [&](f3 rv, float, float4 vj) {
             float r2 = dot(rv, rv);
             float r = sqrtf(r2);
-            float w = kernel_w(r, h);
+            float w = kernel_w_q(div_h(r, h, inv_h, exact), kn);
             f3 vd = sub(xyz(vj), vi);
             sum = add(sum, scale_r(scale(m / vj.w, vd), w));
         });
