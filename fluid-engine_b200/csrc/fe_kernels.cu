@@ -189,7 +189,9 @@ struct RunTable {
 // Per-warp scratch: one form or the other.
 union DensityScratch {
     struct {
-        float4 pos[32];
+        alignas(8) float rx[32];        // the run being tested: its particles' positions
+        alignas(8) float ry[32];
+        alignas(8) float rz[32];
         uint32_t mask[kMaxSlabs][32];
         RunTable table[kCoopRuns];
         uint32_t row[kMaxSlabs * 32];   // the run being tested: its candidates' indices
@@ -247,7 +249,7 @@ __device__ __forceinline__ f3 neighbour_pos(const Bufs& B, uint32_t j, float4& v
 // number of in-range candidates.
 __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& P,
                                                 DensityScratch& S, uint32_t heads, int n_live,
-                                                int cx, int cy, int cz, int& my_table,
+                                                int cx, int cy, int cz, float4 p4, int& my_table,
                                                 uint32_t& n_in) {
     const int lane = lane_id();
     const float h = P.h;
@@ -297,6 +299,11 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
         // the run's row: candidate c of the walk is particle row[c] (each
         // bucket's lane writes its entries)
         for (uint32_t u = 0; u < len; ++u) S.coop.row[excl + u] = start + u;
+        if (mine) {
+            S.coop.rx[lane - r0] = p4.x;
+            S.coop.ry[lane - r0] = p4.y;
+            S.coop.rz[lane - r0] = p4.z;
+        }
         __syncwarp();
         for (uint32_t sl = 0; sl < nslab; ++sl) {
             const uint32_t cidx = (sl << 5) + (uint32_t)lane;
@@ -308,19 +315,20 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
             // against h^2 (1 + 2^-18)); phase 2 applies the exact test.
             // two particles of the run per step in packed FP32 (the test
             // above; the contraction that packing allows is covered by the
-            // widened bound)
+            // widened bound), their coordinates read as pairs from the run's
+            // position arrays
             uint64_t qx2, qy2, qz2;
             asm("mov.b64 %0, {%1, %1};" : "=l"(qx2) : "f"(q.x));
             asm("mov.b64 %0, {%1, %1};" : "=l"(qy2) : "f"(q.y));
             asm("mov.b64 %0, {%1, %1};" : "=l"(qz2) : "f"(q.z));
-            int p = r0;
+            const int cnt = r1 - r0;
+            int p = 0;
 #pragma unroll 1
-            for (; p + 1 < r1; p += 2) {
-                const float4 a0 = S.coop.pos[p], a1 = S.coop.pos[p + 1];
-                uint64_t ax, ay, az, dx, dy, dz, r2;
-                asm("mov.b64 %0, {%1, %2};" : "=l"(ax) : "f"(a0.x), "f"(a1.x));
-                asm("mov.b64 %0, {%1, %2};" : "=l"(ay) : "f"(a0.y), "f"(a1.y));
-                asm("mov.b64 %0, {%1, %2};" : "=l"(az) : "f"(a0.z), "f"(a1.z));
+            for (; p + 1 < cnt; p += 2) {
+                const uint64_t ax = *reinterpret_cast<const uint64_t*>(&S.coop.rx[p]);
+                const uint64_t ay = *reinterpret_cast<const uint64_t*>(&S.coop.ry[p]);
+                const uint64_t az = *reinterpret_cast<const uint64_t*>(&S.coop.rz[p]);
+                uint64_t dx, dy, dz, r2;
                 asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dx) : "l"(ax), "l"(qx2));
                 asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dy) : "l"(ay), "l"(qy2));
                 asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dz) : "l"(az), "l"(qz2));
@@ -332,16 +340,16 @@ __device__ __forceinline__ void coop_candidates(const Bufs& B, const DevParams& 
                 const uint32_t b0 = __ballot_sync(kFull, valid && !(r2a > h2_wide));
                 const uint32_t b1 = __ballot_sync(kFull, valid && !(r2b > h2_wide));
                 if (lane == 0) {
-                    S.coop.mask[sl][p] = b0;
-                    S.coop.mask[sl][p + 1] = b1;
+                    S.coop.mask[sl][r0 + p] = b0;
+                    S.coop.mask[sl][r0 + p + 1] = b1;
                 }
             }
-            if (p < r1) {
-                const float4 a = S.coop.pos[p];
-                const float dx = a.x - q.x, dy = a.y - q.y, dz = a.z - q.z;
+            if (p < cnt) {
+                const float dx = S.coop.rx[p] - q.x, dy = S.coop.ry[p] - q.y,
+                            dz = S.coop.rz[p] - q.z;
                 const float r2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
                 const uint32_t bits = __ballot_sync(kFull, valid && !(r2 > h2_wide));
-                if (lane == 0) S.coop.mask[sl][p] = bits;
+                if (lane == 0) S.coop.mask[sl][r0 + p] = bits;
             }
             __syncwarp();
             if (mine) n_in += __popc(S.coop.mask[sl][lane]);
@@ -382,9 +390,7 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     int my_table = -1;
     uint32_t n1 = 0;
     if (coop) {
-        S.coop.pos[lane] = p4;
-        __syncwarp();
-        coop_candidates(B, P, S, heads, n_live, cx, cy, cz, my_table, n1);
+        coop_candidates(B, P, S, heads, n_live, cx, cy, cz, p4, my_table, n1);
     } else if (live) {
         walk(B, P, pi, [&](uint32_t j, f3, float) {
             if (n1 < (uint32_t)kStage) S.cand[n1][lane] = j;
