@@ -576,8 +576,9 @@ def splat_benchmark(w, local, reps: int = 10):
                          "water_pixels": float((img[..., 3] > 0).mean())}}
 
 
-def run_batch(args, world, rank, local):
-    """The 64 batched dam-break scenes: this rank's LPT share of the scenes in
+def run_batch(args, world, rank, local, w=None):
+    """The batched dam-break scenes (default: 64 scenes of 4k-262k
+    particles; `w`: another batch workload): this rank's LPT share of the scenes in
     one batch context (no collective inside a step), W warm-up frames, then K
     frames timed with CUDA events on the context stream; the time is the max
     over ranks and the value counts every scene's particles (strong scaling:
@@ -590,7 +591,7 @@ def run_batch(args, world, rank, local):
     from fluid_step.pipelines import BatchSimulation, Simulation
     from fluid_step.sharding import run_scene_shard
 
-    w = scene.batch_workload()
+    w = w or scene.batch_workload()
     pos, par = w.positions(), w.params()
     total = int(sum(w.counts))
     clocks = ClockSampler(local)
@@ -655,8 +656,8 @@ def run_batch(args, world, rank, local):
             s_.close()
         out["separate_contexts"] = {"value": total * args.steps / seq,
                                     "ms_per_step": seq * 1e3 / args.steps,
-                                    "timing": "host clock: 64 contexts, one fe_step each per "
-                                              "frame, one stream each"}
+                                    "timing": f"host clock: {len(w.counts)} contexts, one fe_step "
+                                              "each per frame, one stream each"}
     return out
 
 
@@ -719,6 +720,11 @@ def run_gpu(args) -> None:
                 r["learned_over_plain"] = r["plain"]["ms_per_step"] / r["learned"]["ms_per_step"]
             runs[name] = r
     batch = run_batch(args, world, rank, local) if args.batch else None
+    # Many small scenes, where one context per scene is bound by launches:
+    # 256 scenes of 1k-8k particles.
+    batch_small = (run_batch(args, world, rank, local,
+                             scene.batch_workload(n_scenes=256, lo=1024, hi=8192, seed=2))
+                   if args.batch else None)
     splat = splat_benchmark(w, local) if args.full_runs else None
     head = arms["learned"] if "learned" in arms else arms["plain"]
     lib = _abi.load_library()
@@ -809,6 +815,8 @@ def run_gpu(args) -> None:
             out["full_runs"] = runs
         if batch:
             out["batched"] = batch
+        if batch_small:
+            out["batched_small"] = batch_small
         if splat:
             out["density_splat"] = splat
         if "learned" in arms and "plain" in arms:
