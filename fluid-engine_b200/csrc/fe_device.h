@@ -93,7 +93,7 @@ struct Bufs {
     // position, velocity and t with one 256-bit load.
     float4* pa;
     // 32-byte record per particle: pv[2i] = copy of position_b (xyz, written
-    // by reorder), pv[2i+1] = velocity_b with the slot's density in w
+    // by reorder), pv[2i+1] = velocity_b with the slot's m / rho in w
     // (written by density_alpha, kept by the FIXED-mode divergence
     // integration).  Viscosity and the FIXED-mode divergence source fetch a
     // neighbour's position, velocity and density with one 256-bit load.

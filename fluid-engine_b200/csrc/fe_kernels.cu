@@ -140,14 +140,14 @@ __global__ void __launch_bounds__(kBlock) k_snapshot4(float4* dst, const float4*
     dst[i] = v;
 }
 
-// pr = p / rho^2, velocity_b's w = rho and velocity_a's w = the density
+// pr = p / rho^2, velocity_b's w = m / rho and velocity_a's w = the density
 // residual t for all particles (after a host upload of p, rho, position_b or
 // a velocity).  One block per chunk (t needs the scene's rho0).
 __global__ void __launch_bounds__(kBlock) k_refresh_pr(Bufs B) {
     uint32_t i, s, c;
     if (!chunk_of(B, i, s, c)) return;
     posb(B, i)->w = pressure_over_rho2(B.prs[i], B.rho[i]);
-    velb(B, i)->w = B.rho[i];
+    velb(B, i)->w = B.P[s].mass / B.rho[i];
     vela(B, i)->w = density_residual_t(B.rho[i], B.P[s].rho0);
 }
 
@@ -439,9 +439,9 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     }
     if (kDiv) B.src[i] = -a.div;   // divergence_source_term.comp:58-60
     B.rho[i] = a.density;
-    // velocity_b.w carries the density for the neighbour gathers of viscosity
-    // and the FIXED-mode divergence source
-    velb(B, i)->w = a.density;
+    // velocity_b.w carries m / rho (the factor viscosity applies to each
+    // neighbour's velocity, the same division done once per particle)
+    velb(B, i)->w = m / a.density;
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
     B.alpha[i] = al > kEpsR ? al : 0.0f;
     B.nbr_count[i] = a.cnt;
@@ -512,15 +512,15 @@ __device__ __forceinline__ void viscosity_particle(const Bufs& B, uint32_t i, ui
     const f3 pi = xyz(__ldg(posb(B, i)));
     const f3 vi = xyz(__ldg(velb(B, i)));
     f3 sum = {0.0f, 0.0f, 0.0f};
-    // velocity_b.w = rho_j (written by density_alpha): one 256-bit load of the
-    // position/velocity record per neighbour
+    // velocity_b.w = m / rho_j (written by density_alpha): one 256-bit load of
+    // the position/velocity record per neighbour
     for_each_neighbor_pair(
         B, P, i, pi, B.pv, [&](f3 rv, float, float4 vj) {
             float r2 = dot(rv, rv);
             float r = sqrtf(r2);
             float w = kernel_w_q(div_h(r, h, inv_h, exact), kn);
             f3 vd = sub(xyz(vj), vi);
-            sum = add(sum, scale_r(scale(m / vj.w, vd), w));
+            sum = add(sum, scale_r(scale(vj.w, vd), w));
         });
     f3 vv = add(vi, scale(P.visc, sum));
     f3 g = {P.gx, P.gy, P.gz};
