@@ -252,7 +252,7 @@ def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = Fal
     # after-solve bookkeeping and the carry permutation ride in the source,
     # integration and reorder passes
     extra = 2 if learned else 0
-    return 1 + ns + fixed + iters + extra + 1   # + prologue, stats
+    return 1 + ns + fixed + iters + extra   # + prologue (the stats ride in the last integration)
 
 
 # ---------------------------------------------------------------------------

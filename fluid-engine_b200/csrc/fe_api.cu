@@ -702,7 +702,7 @@ fe_status rec_trace(fe_ctx* c, Recorder& R, uint32_t slot) {
 
 // One substep of Renderer::step (renderer/mod.rs:289-337); k = its index in
 // the frame.
-fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
+fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k, bool last) {
     Bufs B = c->B;
     const int fixed = c->fixed_mode() ? 1 : 0;
     fe_status s;
@@ -724,10 +724,20 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k) {
         if ((s = rec_trace(c, R, 2 * k + 1))) return s;
     }
     if ((s = rec_solve(c, R, 1))) return s;
-    if (c->carries())
+    if (last) {   // the frame's stats ride in its last divergence integration
+        if (c->carries())
+            REC(R.k(k_divergence_integration_stats_learn, chunk_grid(c), dim3(kBlock), B, fixed,
+                    c->L, c->upart));
+        else
+            REC(R.k(k_divergence_integration_stats, chunk_grid(c), dim3(kBlock), B, fixed,
+                    c->upart));
+        if (B.n_scenes > 1)  // the per-scene finish, one block per scene
+            REC(R.k(k_stats_finish, dim3(B.n_scenes), dim3(kBlock), B, c->upart));
+    } else if (c->carries()) {
         REC(R.k(k_divergence_integration_learn, chunk_grid(c), dim3(kBlock), B, fixed, c->L));
-    else
+    } else {
         REC(R.k(k_divergence_integration, chunk_grid(c), dim3(kBlock), B, fixed));
+    }
     REC(R.k(k_count_substep, dim3((B.n_scenes + 63) / 64), dim3(64), B));
     return FE_OK;
 }
@@ -740,8 +750,8 @@ fe_status rec_frame(fe_ctx* c, Recorder& R, uint32_t n_substeps, bool init) {
         if ((s = rec_density_alpha(c, R))) return s;
     }
     for (uint32_t k = 0; k < n_substeps; ++k)
-        if ((s = rec_substep(c, R, k))) return s;
-    return rec_stats(c, R);
+        if ((s = rec_substep(c, R, k, k + 1 == n_substeps))) return s;
+    return n_substeps ? FE_OK : rec_stats(c, R);
 }
 
 fe_status need_prepared(fe_ctx* c, const char* what) {

@@ -1011,18 +1011,16 @@ __device__ void stats_finish_scene(Bufs& B, const uint4* upart, uint32_t sc, uin
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upart) {
+// The stats of one chunk (whole block): v = particle i's velocity (the one
+// the pass binds), read by the caller.
+__device__ __forceinline__ void stats_chunk(Bufs B, uint4* upart, bool valid, uint32_t i,
+                                            uint32_t s, uint32_t c, float4 v) {
     __shared__ double smem[8];
     __shared__ uint32_t s_u[3][8];
-    uint32_t i, s, c;
-    bool valid = chunk_of(B, i, s, c);
     const DevParams& P = B.P[s];
-    const float4* vel = fixed ? velb(B, 0) : vela(B, 0);
-    const uint32_t vstride = 2u;
     uint32_t mx = 0, s1 = 0, s2 = 0, bad = 0;
     double d1 = 0.0, d2 = 0.0;
     if (valid) {
-        float4 v = vel[(size_t)i * vstride];
         float speed = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
         mx = __float_as_uint(speed);
         float rho = B.rho[i], src = B.src[i];
@@ -1065,6 +1063,47 @@ __global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upar
         stats_finish_scene(B, upart, 0, 0, smem, s_u);
         if (threadIdx.x == 0) B.G->tickets[kTicketStats] = 0;
     }
+}
+
+__global__ void __launch_bounds__(kBlock) k_stats(Bufs B, int fixed, uint4* upart) {
+    uint32_t i, s, c;
+    const bool valid = chunk_of(B, i, s, c);
+    const float4* vel = fixed ? velb(B, 0) : vela(B, 0);
+    stats_chunk(B, upart, valid, i, s, c,
+                valid ? vel[(size_t)i * 2u] : make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+}
+
+// The substep's last divergence integration and the frame's stats in one
+// pass: the stats read the velocity this pass has just written (the same
+// value the stats pass would read back), and every other input of the stats
+// is final by then.
+template <bool kLearn>
+__device__ __forceinline__ void divergence_integration_stats_body(const Bufs& B, int fixed,
+                                                                  const LearnArgs& L,
+                                                                  uint4* upart) {
+    uint32_t i, s, c;
+    const bool valid = chunk_of(B, i, s, c);
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (valid) {
+        const DevParams& P = B.P[s];
+        float4* vel = fixed ? velb(B, i) : vela(B, i);
+        const float4 v0 = *vel;
+        const f3 nv = add(xyz(v0), scale_r(xyz(*accp(B, i)), P.dt));
+        v = make_float4(nv.x, nv.y, nv.z, v0.w);
+        *vel = v;
+        if (kLearn) after_solve_particle(B, L, P, i, 1);
+    }
+    stats_chunk(B, upart, valid, i, s, c, v);
+}
+
+__global__ void __launch_bounds__(kBlock) k_divergence_integration_stats(Bufs B, int fixed,
+                                                                         uint4* upart) {
+    divergence_integration_stats_body<false>(B, fixed, LearnArgs{}, upart);
+}
+__global__ void __launch_bounds__(kBlock) k_divergence_integration_stats_learn(Bufs B, int fixed,
+                                                                               LearnArgs L,
+                                                                               uint4* upart) {
+    divergence_integration_stats_body<true>(B, fixed, L, upart);
 }
 
 __global__ void __launch_bounds__(kBlock) k_stats_finish(Bufs B, uint4* upart) {

@@ -51,6 +51,10 @@ __global__ void k_pressure_integration_learn(Bufs B, LearnArgs L);
 __global__ void k_divergence_integration(Bufs B, int fixed);
 __global__ void k_divergence_integration_learn(Bufs B, int fixed, LearnArgs L);
 __global__ void k_stats(Bufs B, int fixed, uint4* upart);
+// The last substep's divergence integration with the frame's stats fused in.
+__global__ void k_divergence_integration_stats(Bufs B, int fixed, uint4* upart);
+__global__ void k_divergence_integration_stats_learn(Bufs B, int fixed, LearnArgs L,
+                                                     uint4* upart);
 __global__ void k_frame_prologue(Bufs B);
 __global__ void k_count_substep(Bufs B);
 template <int kThreads, bool kPersist>
