@@ -218,23 +218,7 @@ __device__ __forceinline__ void epilogue_silu64(uint32_t taddr, const float* bia
     }
 }
 
-// ---------------------------------------------------------------------------
-// Inference: out[i][0..1] = MLP(x_i) for n rows of X (BF16, 16 per row).
-// 256 threads: warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows) and
-// column half w / 4 of each accumulator.  64 TMEM columns are reused by the
-// three layers and one shared buffer holds both hidden activations (each
-// product has finished reading it before the next epilogue overwrites it),
-// so several blocks share an SM.
-// ---------------------------------------------------------------------------
 constexpr int kInferThreads = 256;
-
-struct InferSmem {
-    SmemWeights W;
-    alignas(128) uint8_t x[kTile * 16 * 2];
-    alignas(128) uint8_t h[kTile * 64 * 2];
-    alignas(8) uint64_t bar;
-    uint32_t tmem_base;
-};
 
 __device__ __forceinline__ uint32_t lane_addr8(uint32_t base, uint32_t col) {
     uint32_t warp = threadIdx.x >> 5;
@@ -269,17 +253,35 @@ __device__ __forceinline__ void epilogue_half(uint32_t taddr, uint32_t c0, const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Inference: out[i][0..1] = MLP(x_i) for n rows of X (BF16, 16 per row),
+// on pairs of 128-row tiles: a block of 256 threads takes tiles 2p and
+// 2p + 1 together (accumulators in TMEM columns [0, 64) and [64, 128));
+// warps 0-3 serve the first tile's rows and warps 4-7 the second's, each
+// warp all 64 columns of its 32 rows.  Each barrier and product round trip
+// then serves 256 rows, and four blocks per SM keep eight tiles in flight.
+// With kApply the epilogue also starts solve A.which from the output it has
+// just written (warm_apply_particle).
+// ---------------------------------------------------------------------------
+struct InferPairSmem {
+    SmemWeights W;
+    alignas(128) uint8_t x[2][kTile * 16 * 2];
+    alignas(128) uint8_t h[2][kTile * 64 * 2];
+    alignas(8) uint64_t bar;
+    uint32_t tmem_base;
+};
+constexpr int kInferPairMaxCtasPerSm = 4;   // 4 x 128 TMEM columns fill an SM
+
 template <bool kApply>
-__global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
-                                                             const __nv_bfloat16* __restrict__ X,
-                                                             float* __restrict__ out, uint32_t n,
-                                                             uint32_t* error_flags, ApplyArgs A) {
+__global__ void __launch_bounds__(kInferThreads) k_mlp_infer_pair(
+    Params P, const __nv_bfloat16* __restrict__ X, float* __restrict__ out, uint32_t n,
+    uint32_t* error_flags, ApplyArgs A) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw);
+    InferPairSmem& S = *reinterpret_cast<InferPairSmem*>(smem_raw);
     const uint32_t tid = threadIdx.x;
     const uint32_t warp = tid >> 5, lane = tid & 31u;
+    const uint32_t sub = warp >> 2;                  // the tile of the pair this warp serves
     const uint32_t row = (warp & 3u) * 32u + lane;   // TMEM lane = sample row
-    const uint32_t half = (warp >> 2) * 32u;         // column half
     for (int t = tid; t < 64 * 16; t += kInferThreads)
         *reinterpret_cast<__nv_bfloat16*>(S.W.w1 + off_k(t / 16, t % 16, 16)) = P.w1[t];
     for (int t = tid; t < 64 * 64; t += kInferThreads)
@@ -295,74 +297,82 @@ __global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
     }
     if (tid < 16) S.W.b3[tid] = tid < 2 ? P.b3[tid] : 0.0f;
     if (tid == 0) bar_init(&S.bar);
-    tmem_alloc(&S.tmem_base, 64);
+    tmem_alloc(&S.tmem_base, 128);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     const uint32_t d = S.tmem_base;
+    const uint32_t ta = lane_addr8(d, 64u * sub);
     uint32_t phase = 0;
     bool ok = true;
-    const uint32_t ntiles = (n + kTile - 1) / kTile;
-    const uint64_t dx = desc(smem_u32(S.x), 128, 256);
+    const uint32_t npairs = (n + 2 * kTile - 1) / (2 * kTile);
     const uint64_t dw1 = desc(smem_u32(S.W.w1), 128, 256);
-    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        // X tile: 16 bytes per thread (row tid / 2, half tid % 2).
-        {
+    for (uint32_t pr = blockIdx.x; pr < npairs && ok; pr += gridDim.x) {
+        // X rows of both tiles: 16 bytes per thread and step (row tid / 2,
+        // half tid % 2), two steps
+        for (uint32_t q = 0; q < 2; ++q) {
             const uint32_t r = tid >> 1, part = tid & 1u;
-            const uint32_t g = tile * kTile + r;
+            const uint32_t g = (2 * pr + q) * kTile + r;
             uint4 a = make_uint4(0, 0, 0, 0);
             if (g < n) a = reinterpret_cast<const uint4*>(X + (size_t)g * 16)[part];
-            *reinterpret_cast<uint4*>(S.x + off_k(r, part * 8, 16)) = a;
+            *reinterpret_cast<uint4*>(S.x[q] + off_k(r, part * 8, 16)) = a;
         }
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
         if (tid == 0) {
             tc_after_sync();
-            mma(d, dx, dw1, idesc(128, 64, 0, 0), 0);
+            for (uint32_t q = 0; q < 2; ++q)
+                mma(d + 64u * q, desc(smem_u32(S.x[q]), 128, 256), dw1, idesc(128, 64, 0, 0), 0);
             commit(&S.bar);
         }
         ok = __syncthreads_and(bar_wait(&S.bar, phase));
         phase ^= 1;
         tc_after_sync();
-        if (ok) epilogue_half(lane_addr8(d, 0), half, S.W.b1, S.h, row);
+        if (ok) {
+            epilogue_half(ta, 0, S.W.b1, S.h[sub], row);
+            epilogue_half(ta, 32, S.W.b1, S.h[sub], row);
+        }
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
         if (tid == 0 && ok) {
             tc_after_sync();
-            for (uint32_t kk = 0; kk < 4; ++kk)
-                mma(d, desc(smem_u32(S.h) + kk * 256, 128, 1024),
-                    desc(smem_u32(S.W.w2) + kk * 256, 128, 1024), idesc(128, 64, 0, 0), kk > 0);
+            for (uint32_t q = 0; q < 2; ++q)
+                for (uint32_t kk = 0; kk < 4; ++kk)
+                    mma(d + 64u * q, desc(smem_u32(S.h[q]) + kk * 256, 128, 1024),
+                        desc(smem_u32(S.W.w2) + kk * 256, 128, 1024), idesc(128, 64, 0, 0), kk > 0);
             commit(&S.bar);
         }
         ok = __syncthreads_and(ok && bar_wait(&S.bar, phase));
         phase ^= 1;
         tc_after_sync();
-        if (ok) epilogue_half(lane_addr8(d, 0), half, S.W.b2, S.h, row);
+        if (ok) {
+            epilogue_half(ta, 0, S.W.b2, S.h[sub], row);
+            epilogue_half(ta, 32, S.W.b2, S.h[sub], row);
+        }
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
         if (tid == 0 && ok) {
             tc_after_sync();
-            for (uint32_t kk = 0; kk < 4; ++kk)
-                mma(d, desc(smem_u32(S.h) + kk * 256, 128, 1024),
-                    desc(smem_u32(S.W.w3) + kk * 256, 128, 1024), idesc(128, 16, 0, 0), kk > 0);
+            for (uint32_t q = 0; q < 2; ++q)
+                for (uint32_t kk = 0; kk < 4; ++kk)
+                    mma(d + 64u * q, desc(smem_u32(S.h[q]) + kk * 256, 128, 1024),
+                        desc(smem_u32(S.W.w3) + kk * 256, 128, 1024), idesc(128, 16, 0, 0), kk > 0);
             commit(&S.bar);
         }
         ok = __syncthreads_and(ok && bar_wait(&S.bar, phase));
         phase ^= 1;
         tc_after_sync();
-        if (ok && half == 0) {
+        if (ok) {
             float v[16];
-            tmem_ld16(lane_addr8(d, 0), v);
-            const uint32_t g = tile * kTile + row;
+            tmem_ld16(ta, v);
+            const uint32_t g = (2 * pr + sub) * kTile + row;
             if (g < n) {
                 const float o0 = v[0] + S.W.b3[0], o1 = v[1] + S.W.b3[1];
                 reinterpret_cast<float2*>(out)[g] = make_float2(o0, o1);
-                // the solve's start from this output (the same value the
-                // stand-alone pass would read back from `out`)
                 if (kApply)
                     warm_apply_particle(A.B, A.L, A.B.P[scene_of(A.B, g)], g, A.which,
                                         A.which == 0 ? o0 : o1);
@@ -376,7 +386,7 @@ __global__ void __launch_bounds__(kInferThreads) k_mlp_infer(Params P,
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
-    tmem_free(d, 64);
+    tmem_free(d, 128);
 }
 
 // ---------------------------------------------------------------------------
@@ -669,19 +679,21 @@ __global__ void k_adam(float* __restrict__ master, float* __restrict__ grad, flo
 
 }  // namespace
 
-size_t infer_smem_bytes() { return sizeof(InferSmem) + 1024; }
+size_t infer_smem_bytes() { return sizeof(InferPairSmem) + 1024; }
 size_t train_smem_bytes() { return sizeof(TrainSmem) + 1024; }
 
 cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out, int ctas_per_sm,
                          bool apply) {
     size_t smem = infer_smem_bytes();
-    const void* func = apply ? (const void*)k_mlp_infer<true> : (const void*)k_mlp_infer<false>;
+    const void* func =
+        apply ? (const void*)k_mlp_infer_pair<true> : (const void*)k_mlp_infer_pair<false>;
     cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     if (ctas_per_sm < 1 || ctas_per_sm > kInferMaxCtasPerSm) return cudaErrorInvalidValue;
-    uint32_t tiles = (n + kTile - 1) / kTile;
-    const uint32_t cap = (uint32_t)(num_sms * ctas_per_sm);
+    const int cps = ctas_per_sm < kInferPairMaxCtasPerSm ? ctas_per_sm : kInferPairMaxCtasPerSm;
+    uint32_t tiles = (n + 2 * kTile - 1) / (2 * kTile);   // pairs of tiles
+    const uint32_t cap = (uint32_t)(num_sms * cps);
     uint32_t grid = tiles < cap ? tiles : cap;
     out->func = func;
     out->grid = dim3(grid > 0 ? grid : 1);
@@ -696,8 +708,8 @@ cudaError_t infer(const Params& P, const __nv_bfloat16* X, float* out, uint32_t 
     KernelLaunch L;
     cudaError_t e = infer_launch(n, num_sms, &L, ctas_per_sm);
     if (e != cudaSuccess) return e;
-    k_mlp_infer<false><<<L.grid, L.block, L.smem, stream>>>(P, X, out, n, error_flags,
-                                                            ApplyArgs{});
+    k_mlp_infer_pair<false><<<L.grid, L.block, L.smem, stream>>>(P, X, out, n, error_flags,
+                                                                 ApplyArgs{});
     return cudaGetLastError();
 }
 

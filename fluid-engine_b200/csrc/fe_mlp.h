@@ -60,10 +60,11 @@ struct KernelLaunch {
     dim3 grid, block;
     size_t smem;
 };
-// Inference grid: min(tiles, num_sms * ctas_per_sm) blocks of 256 threads
-// looping over 128-row tiles.  Shared memory and registers allow up to
-// kInferMaxCtasPerSm blocks per SM.
-constexpr int kInferDefaultCtasPerSm = 6;
+// Inference grid: min(pairs of 128-row tiles, num_sms * ctas_per_sm) blocks
+// of 256 threads looping over the pairs.  ctas_per_sm is accepted in
+// 1..kInferMaxCtasPerSm; each block holds 128 TMEM columns, so at most 4
+// run on an SM and larger values act as 4.
+constexpr int kInferDefaultCtasPerSm = 4;
 constexpr int kInferMaxCtasPerSm = 6;
 cudaError_t infer_launch(uint32_t n, int num_sms, KernelLaunch* out,
                          int ctas_per_sm = kInferDefaultCtasPerSm, bool apply = false);

@@ -20,7 +20,7 @@
 
 namespace fe {
 
-const int kMlpCtaChoices[kMlpCtaCandidates] = {2, 3, 4, 6};
+const int kMlpCtaChoices[kMlpCtaCandidates] = {1, 2, 3, 4};
 
 namespace {
 

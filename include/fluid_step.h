@@ -489,7 +489,7 @@ FE_API fe_status fe_sort_flags(uint32_t* flags_out, void* stream);
  *   radix_digit_bits, radix_items: onesweep digit width (8 or 10) and keys
  *     per thread (4, 8, 16; the pairs (8,4) (8,8) (8,16) (10,8) (10,16)).
  *   mlp_ctas_per_sm: blocks per SM of the learned warm start's inference
- *     grid (1..6).
+ *     grid (1..6; at most 4 fit on an SM, larger values act as 4).
  *   nbr_threads[g]: threads per block of neighbour group g, 128, 256 or 512
  *     (a block covers half a 256-particle chunk per pass, one chunk, or two
  *     chunks at a time; particles per thread = 256 / threads per chunk);
