@@ -1772,6 +1772,7 @@ static fe_status ensure_learn_buffers(fe_ctx* c) {
     if ((s = dev_alloc(c, &carry, c->n))) return s;
     c->L.xb = xb;
     FE_CUDA(cudaMemsetAsync(c->L.mom, 0, (size_t)c->n * 16, c->stream));
+    FE_CUDA(cudaMemsetAsync(c->L.mom_tmp, 0, (size_t)c->n * 16, c->stream));
     FE_CUDA(cudaMemsetAsync(carry, 0, (size_t)c->n * 16, c->stream));
     // no capture slot yet: w = all ones
     FE_CUDA(cudaMemset2DAsync(reinterpret_cast<char*>(carry) + 12, 16, 0xFF, 4, c->n, c->stream));

@@ -125,7 +125,9 @@ struct Bufs {
 //   (feature 11), w = capture slot of the solve in progress (bits; ~0 none).
 // mom[i] = features 7..10 (the first four moments), with z above the
 // moments the density source computed at the substep's start; the
-// divergence solve's features reuse them after the mid-substep re-sort.
+// divergence solve's features reuse them after the mid-substep re-sort,
+// reading the re-sorted copy mom_tmp (nothing reads mom again before the
+// next density source rewrites it, so it is not copied back).
 struct LearnArgs {
     const float* norm;          // model standardisation: x mean[12], std[12], y mean[2], std[2]
     void* xb;                   // BF16 feature rows [n][16] (network input)

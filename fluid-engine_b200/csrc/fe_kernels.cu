@@ -116,7 +116,6 @@ __device__ __forceinline__ void take_pressure_body(const Bufs& B, const LearnArg
     posb(B, i)->w = pressure_over_rho2(p, B.rho[i]);
     if (kCarry) {
         L.carry[i] = L.carry_tmp[i];
-        L.mom[i] = L.mom_tmp[i];
     }
 }
 
@@ -448,7 +447,8 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     posb(B, i)->w = pressure_over_rho2(B.prs[i], a.density);
     if (a.cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
     if (kLearn) {
-        const float4 m4 = L.mom[i];
+        // the substep's density-source moments, as the re-sort gathered them
+        const float4 m4 = L.mom_tmp[i];
         const float fm[kMoments] = {m4.x, m4.y, m4.z, m4.w, L.carry[i].z};
         emit_features(B, L, P, i, s, 1, a.div, vi, fm);
     }

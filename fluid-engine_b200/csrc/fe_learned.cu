@@ -26,7 +26,6 @@ __global__ void __launch_bounds__(kBlock) k_carry_take(Bufs B, LearnArgs L) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
     L.carry[i] = L.carry_tmp[i];
-    L.mom[i] = L.mom_tmp[i];
 }
 
 }  // namespace fe
