@@ -224,7 +224,8 @@ fe_status validate(const fe_params* p) {
 // Whether, for the divisor b, the reciprocal step of div_h (fe_common.cuh)
 // returns the correctly rounded r / b for every significand of r: checked
 // over the 2^23 floats of [1, 2), since every step scales exactly with r's
-// exponent.  About 20 ms per new b; the answer is kept per b.
+// exponent.  About 50 ms per new b on one host core; the answer is kept
+// per b.
 bool recip_division_exact(float b) {
     if (!(b > 0.0f) || !std::isfinite(b) || !std::isnormal(b) || !std::isnormal(1.0f / b))
         return false;
