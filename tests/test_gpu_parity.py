@@ -188,6 +188,9 @@ CASES = {
                        divergence_error_pct=5.0),
     "bitonic": dict(sort_algorithm=_abi.FE_SORT_BITONIC),
     "cfl_reference": dict(use_cfl=1, dt=0.005),
+    # another smoothing radius: the r / h reciprocal step is checked for it
+    # anew, and more particles overflow the 64-entry list into the walk
+    "radius_0p12": dict(smoothing_radius=0.12),
 }
 
 
