@@ -622,9 +622,10 @@ struct State : Base {
         }
     }
 
-    // k_warm_apply (fe_learned.cu): the solve's start from the network's
-    // output, clamped to [0, max(d_i, carried density kappa)]; particles with
-    // fewer than 16 neighbours keep the plain start.
+    // warm_apply_particle (fe_features.cuh, run in the network's epilogue):
+    // the solve's start from the network's output, clamped to
+    // [0, max(d_i, carried density kappa)]; particles with fewer than 16
+    // neighbours keep the plain start.
     void warm_apply(int which) override {
         uint32_t slot = 2u * cur_substep + (uint32_t)which;
         if (slot >= net_slots) {
