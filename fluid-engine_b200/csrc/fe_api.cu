@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <utility>
 #include <string>
@@ -221,11 +222,26 @@ fe_status validate(const fe_params* p) {
     return FE_OK;
 }
 
-// Whether, for the divisor b, the reciprocal step of div_h (fe_common.cuh)
-// returns the correctly rounded r / b for every significand of r: checked
-// over the 2^23 floats of [1, 2), since every step scales exactly with r's
-// exponent.  About 50 ms per new b on one host core; the answer is kept
-// per b.
+// Whether the reciprocal step of div_h (fe_common.cuh) returns the correctly
+// rounded r / b for every significand m of r in [lo, hi) of [0, 2^23).
+bool recip_division_exact_range(float b, uint32_t lo, uint32_t hi) {
+    const float y = 1.0f / b;
+    for (uint32_t m = lo; m < hi; ++m) {
+        const uint32_t ab = 0x3f800000u | m;
+        float a;
+        std::memcpy(&a, &ab, 4);
+        const float ref = a / b;
+        const float q0 = a * y;
+        const float q = std::fmaf(std::fmaf(-q0, b, a), y, q0);
+        if (std::memcmp(&ref, &q, 4) != 0) return false;
+    }
+    return true;
+}
+
+// Whether, for the divisor b, that step is exact for every significand of r:
+// checked over the 2^23 floats of [1, 2), since every step scales exactly
+// with r's exponent.  About 50 ms of host time per new b, spread over up to
+// 16 threads; the answer is kept per b.
 bool recip_division_exact(float b) {
     if (!(b > 0.0f) || !std::isfinite(b) || !std::isnormal(b) || !std::isnormal(1.0f / b))
         return false;
@@ -236,17 +252,18 @@ bool recip_division_exact(float b) {
     std::lock_guard<std::mutex> lock(mu);
     for (const auto& kv : known)
         if (kv.first == key) return kv.second;
-    const float y = 1.0f / b;
+    const uint32_t total = 1u << 23;
+    const uint32_t nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<char> ok(nt, 0);
+    std::vector<std::thread> pool;
+    for (uint32_t t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            ok[t] = recip_division_exact_range(b, (uint32_t)((uint64_t)total * t / nt),
+                                               (uint32_t)((uint64_t)total * (t + 1) / nt));
+        });
+    for (auto& th : pool) th.join();
     bool exact = true;
-    for (uint32_t m = 0; m < (1u << 23) && exact; ++m) {
-        const uint32_t ab = 0x3f800000u | m;
-        float a;
-        std::memcpy(&a, &ab, 4);
-        const float ref = a / b;
-        const float q0 = a * y;
-        const float q = std::fmaf(std::fmaf(-q0, b, a), y, q0);
-        exact = std::memcmp(&ref, &q, 4) == 0;
-    }
+    for (char v : ok) exact = exact && v;
     known.emplace_back(key, exact);
     return exact;
 }
