@@ -203,22 +203,31 @@ struct DensityAcc {
     f3 grad_sum = {0.0f, 0.0f, 0.0f};
     uint32_t cnt = 0;
     float div = 0.0f;   // kDiv: the divergence source's sum
+    uint2* op = nullptr;   // the particle's next list slot
 };
 
-// kn = kernel_norm(h); q = r / h is shared by W and grad W.  kDiv != 0 also
+// kn = kernel_norm(h); q = r / h is shared by W and grad W.  The list entry
+// goes to a.op, the particle's next slot (a.op advances by one row).  kDiv != 0 also
 // sums divergence_source_term.comp's m (v_i - v_j) . grad W over the same
 // pairs in the same order (vi, vj: the velocities that pass binds).
 template <int kDiv>
 __device__ __forceinline__ void density_term(DensityAcc& a, float m, const DevParams& P, float kn,
-                                             uint32_t j, f3 rv, float r2, uint2* out,
-                                             uint32_t stride, f3 vi, float4 vj) {
+                                             uint32_t j, f3 rv, float r2, uint32_t stride,
+                                             f3 vi, float4 vj) {
     const float h = P.h;
     float r = sqrtf(r2);
     float q = div_h(r, h, P.inv_h, P.h_recip_exact);
     float w = kernel_w_q(q, kn);
     a.density += m * w;
     if (r > kEpsR) {
-        float g = kernel_grad_scale_q(q, r, h, kn);
+        float g = 0.0f;   // kernel_grad_scale_q with r > 1e-6 known
+        if (!(q >= 1.0f)) {
+            const float inner = kn * (18.0f * q * q - 12.0f * q);
+            const float omq = 1.0f - q;
+            const float outer = kn * -6.0f * omq * omq;
+            const float gf = q <= 0.5f ? inner : outer;
+            g = gf / (h * r);
+        }
         f3 grad = scale(g, rv);
         f3 mg = scale(m, grad);
         a.grad_sum = add(a.grad_sum, mg);
@@ -227,7 +236,10 @@ __device__ __forceinline__ void density_term(DensityAcc& a, float m, const DevPa
             f3 vd = sub(vi, xyz(vj));
             a.div += m * dot(vd, grad);
         }
-        if (a.cnt < kNbrCap) out[(size_t)a.cnt * stride] = make_uint2(j, __float_as_uint(g));
+        if (a.cnt < kNbrCap) {
+            *a.op = make_uint2(j, __float_as_uint(g));
+            a.op += stride;
+        }
         ++a.cnt;
     }
 }
@@ -402,6 +414,7 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     uint2* out = B.nbr + i;
     const uint32_t stride = B.n_total;
     DensityAcc a;
+    a.op = out;
     const f3 vi = kDiv ? xyz(__ldg(kDiv == 1 ? velb(B, i) : vela(B, i))) : f3{0.0f, 0.0f, 0.0f};
     float4 vj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (coop && my_table >= 0) {
@@ -422,18 +435,18 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
             f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
             const float r2 = dot(rv, rv);
             if (r2 > h * h) continue;   // the shader's test (phase 1 passed a superset)
-            density_term<kDiv>(a, m, P, kn, j, rv, r2, out, stride, vi, vj);
+            density_term<kDiv>(a, m, P, kn, j, rv, r2, stride, vi, vj);
         }
     } else if (!coop && n1 <= (uint32_t)kStage) {
         for (uint32_t k = 0; k < n1; ++k) {
             uint32_t j = S.cand[k][lane];
             f3 rv = sub(pi, neighbour_pos<kDiv>(B, j, vj));
-            density_term<kDiv>(a, m, P, kn, j, rv, dot(rv, rv), out, stride, vi, vj);
+            density_term<kDiv>(a, m, P, kn, j, rv, dot(rv, rv), stride, vi, vj);
         }
     } else {
         walk(B, P, pi, [&](uint32_t j, f3 rv, float r2) {
             if (kDiv) vj = __ldg(kDiv == 1 ? velb(B, j) : vela(B, j));
-            density_term<kDiv>(a, m, P, kn, j, rv, r2, out, stride, vi, vj);
+            density_term<kDiv>(a, m, P, kn, j, rv, r2, stride, vi, vj);
         });
     }
     if (kDiv) B.src[i] = -a.div;   // divergence_source_term.comp:58-60
