@@ -239,9 +239,9 @@ def barrier(world: int):
 def launches_per_frame(stats, passes: int, fixed_mode: bool, learned: bool = False) -> float:
     """Kernels of one frame with one substep (the frame graph's nodes)."""
     # neighbour search: hash, scratch fill, histogram, P passes, table fill,
-    # offsets, reorder (+ pressure carry in FIXED mode, + learned state)
-    ns = 1 + 1 + 1 + passes + 1 + 1 + 1 + (1 if fixed_mode else 0) + \
-        (1 if learned and not fixed_mode else 0)
+    # offsets, reorder (density_alpha takes the gathered pressure and
+    # learned state current)
+    ns = 1 + 1 + 1 + passes + 1 + 1 + 1
     # viscosity, density source, 2 x (solve begin + end), integration,
     # density/alpha (with the divergence source summed in), divergence
     # integration, substep counter

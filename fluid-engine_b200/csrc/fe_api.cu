@@ -588,8 +588,11 @@ fe_status rec_list_pass(fe_ctx* c, Recorder& R, int pass) {
     }
 }
 
-// NeighborSearch::execute (neighbor_search.rs:176-231).
-fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
+// NeighborSearch::execute (neighbor_search.rs:176-231).  take: end with the
+// copy that makes the gathered pressures (FIXED mode) and learned carry
+// current; the substep's search leaves it to density_alpha_div, which runs
+// next and does it per particle.
+fe_status rec_neighbor_search(fe_ctx* c, Recorder& R, bool take = true) {
     Bufs B = c->B;
     const bool radix = c->sort_algorithm() == FE_SORT_RADIX;
     uint32_t passes = radix_passes(c->key_bits, c->radix_cfg.digit_bits);
@@ -617,13 +620,14 @@ fe_status rec_neighbor_search(fe_ctx* c, Recorder& R) {
     if (c->carries()) {
         // the learned state rides along with the gather and the copy-back
         REC(R.k(k_reorder_carry, flat_grid(c->n), dim3(kBlock), B, fixed, c->L));
+        if (!take) return FE_OK;
         if (fixed)
             REC(R.k(k_take_pressure_carry, flat_grid(c->n), dim3(kBlock), B, c->L));
         else
             REC(R.k(k_carry_take, flat_grid(c->n), dim3(kBlock), B, c->L));
     } else {
         REC(R.k(k_reorder, flat_grid(c->n), dim3(kBlock), B, fixed));
-        if (fixed) REC(R.k(k_take_pressure, flat_grid(c->n), dim3(kBlock), B));
+        if (fixed && take) REC(R.k(k_take_pressure, flat_grid(c->n), dim3(kBlock), B));
     }
     return FE_OK;
 }
@@ -735,7 +739,7 @@ fe_status rec_substep(fe_ctx* c, Recorder& R, uint32_t k, bool last) {
         REC(R.k(k_pressure_integration_learn, chunk_grid(c), dim3(kBlock), B, c->L));
     else if ((s = rec_simple(c, R, k_pressure_integration)))
         return s;
-    if ((s = rec_neighbor_search(c, R))) return s;
+    if ((s = rec_neighbor_search(c, R, false))) return s;
     if ((s = rec_density_alpha_div(c, R))) return s;
     if (c->learned()) {   // ... and the divergence solve
         if ((s = rec_mlp(c, R, 1))) return s;

@@ -457,12 +457,24 @@ __device__ __forceinline__ void density_alpha_particle(const Bufs& B, DensityScr
     float al = a.sum_grad_sq + dot(a.grad_sum, a.grad_sum);
     B.alpha[i] = al > kEpsR ? al : 0.0f;
     B.nbr_count[i] = a.cnt;
-    posb(B, i)->w = pressure_over_rho2(B.prs[i], a.density);
+    // After the substep's re-sort this pass also makes the gathered state
+    // current (what a separate copy pass did before): FIXED mode's pressure,
+    // and the learned warm start's carry.
+    float p_i;
+    if (kDiv == 1) {
+        p_i = B.prs_tmp[i];
+        B.prs[i] = p_i;
+    } else {
+        p_i = B.prs[i];
+    }
+    posb(B, i)->w = pressure_over_rho2(p_i, a.density);
     if (a.cnt > kNbrCap) atomicOr(&B.G->flags, 0x2u);
     if (kLearn) {
+        const float4 cr = L.carry_tmp[i];
+        L.carry[i] = cr;
         // the substep's density-source moments, as the re-sort gathered them
         const float4 m4 = L.mom_tmp[i];
-        const float fm[kMoments] = {m4.x, m4.y, m4.z, m4.w, L.carry[i].z};
+        const float fm[kMoments] = {m4.x, m4.y, m4.z, m4.w, cr.z};
         emit_features(B, L, P, i, s, 1, a.div, vi, fm);
     }
 }
@@ -480,7 +492,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>) k_density_alph
 // summed in its pair loop: the divergence source needs exactly these pairs,
 // gradients and order, and the neighbour's velocity shares a 32-byte record
 // with the position copy the loop loads.  fixed: FIXED mode (velocity_b),
-// else REFERENCE mode (velocity_a).
+// else REFERENCE mode (velocity_a).  It runs right after the substep's
+// re-sort and takes over that search's last copy: FIXED mode's gathered
+// pressures (prs_tmp) become current here.
 template <int kThreads, bool kPersist>
 __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
     k_density_alpha_div(Bufs B, int fixed) {
@@ -497,7 +511,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
     }
 }
 
-// The same with the learned state: also the divergence solve's features.
+// The same with the learned state: also the divergence solve's features,
+// and the gathered carry (carry_tmp) becomes current here in both modes.
 template <int kThreads, bool kPersist>
 __global__ void __launch_bounds__(kThreads, kMinBlocks<kThreads>)
     k_density_alpha_div_learn(Bufs B, int fixed, LearnArgs L) {

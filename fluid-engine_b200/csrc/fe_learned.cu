@@ -21,7 +21,8 @@
 namespace fe {
 
 // Copies the re-sorted learned state back (k_reorder_carry gathered it into
-// carry_tmp); FIXED mode does this inside k_take_pressure_carry.
+// carry_tmp); FIXED mode does this inside k_take_pressure_carry, and after a
+// substep's re-sort k_density_alpha_div_learn does it.
 __global__ void __launch_bounds__(kBlock) k_carry_take(Bufs B, LearnArgs L) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= B.n_total) return;
