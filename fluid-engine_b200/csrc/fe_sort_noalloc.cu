@@ -3,11 +3,9 @@
 //
 // fe_sort_pairs allocates scratch the first time it sees a size.  Some
 // callers cannot accept that: a frame loop that must never stall (cudaMalloc
-// and cudaFree synchronise the whole device), code recording work into a CUDA
-// graph through stream capture in global mode (allocation calls are refused
-// while such a capture is open), and host applications that budget every byte
-// of device memory themselves and forbid libraries to allocate behind their
-// back.  fe_sort_pairs_noalloc sorts with a scratch area that is a file-scope
+// and cudaFree synchronise the whole device), and host applications that
+// budget every byte of device memory themselves and forbid libraries to
+// allocate behind their back.  fe_sort_pairs_noalloc sorts with a scratch area that is a file-scope
 // __device__ array: the CUDA runtime reserves it on each GPU when the library
 // is loaded there, and it stays reserved until the process exits.
 #include <cuda.h>

@@ -629,9 +629,8 @@ FE_API fe_status fe_debug_read_trace(fe_ctx* ctx, uint32_t slot, uint16_t* rows,
 
 /* Radix sort that allocates nothing.  No counterpart in the reference: it is
  * for callers that cannot let a library allocate device memory — a frame
- * loop that must not stall (cudaMalloc/cudaFree synchronise the device),
- * work recorded by stream capture in global mode (allocation is refused while
- * such a capture is open), or a host that budgets all device memory itself.
+ * loop that must not stall (cudaMalloc/cudaFree synchronise the device), or
+ * a host that budgets all device memory itself.
  * Same result as fe_sort_pairs with FE_SORT_RADIX.  Its scratch is a static
  * device array of about 9 MiB that every GPU loading the library holds until
  * the process exits; n above FE_SORT_NOALLOC_MAX_PAIRS returns

@@ -1,8 +1,8 @@
 """fe_sort_pairs_noalloc: the radix sort that allocates no device memory.
 
 Some callers cannot let the library allocate: a frame loop that must not
-stall (cudaMalloc/cudaFree synchronise the device), work recorded by stream
-capture in global mode, or a host that budgets all device memory itself.  For
+stall (cudaMalloc/cudaFree synchronise the device), or a host that budgets
+all device memory itself.  For
 them the sort's scratch is a static device array of the library.  This test
 calls the entry point through the C ABI twice in a row, with different sizes
 and key widths (so a stale scratch from the first call would show in the
