@@ -742,27 +742,40 @@ def run_gpu(args) -> None:
     achieved = alg / (kern[dom] / 1e3) / 1e9
     traffic = None
     warp_inst = None
+    fp32_inst = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
         if dom in tj and tj[dom].get("workload") == args.workload:
             traffic = tj[dom]["dram_bytes_per_launch"]
             warp_inst = tj[dom].get("warp_instructions_per_launch")
+            fp32_inst = tj[dom].get("fp32_thread_instructions_per_launch")
     except Exception:
         pass
+    mhz = (head["clocks"] or {}).get("sm_mhz") or 1965.0
     # The neighbour-walk kernels are bound by instruction issue, not by HBM:
     # warp instructions per launch (ncu smsp__inst_executed.sum) over the
     # launch time, against 148 SMs x 4 schedulers x one issue per cycle at
     # the SM clock sampled during the run.
     issue = None
     if warp_inst:
-        mhz = (head["clocks"] or {}).get("sm_mhz") or 1965.0
         issue_peak = 148 * 4 * mhz * 1e6
         issue_achieved = warp_inst / (kern[dom] / 1e3)
         issue = {"kernel": dom, "warp_instructions_per_launch": warp_inst,
                  "achieved": issue_achieved, "peak": issue_peak, "unit": "warp-inst/s",
                  "frac": issue_achieved / issue_peak,
                  "source": "instruction count from profiles/traffic.json (ncu)"}
+    # FP32 fraction of the same kernel: FP32 thread instructions per launch
+    # (ncu sm__sass_thread_inst_executed_op_fp32_pred_on.sum) over the launch
+    # time, against 148 SMs x 128 FP32 lanes x one instruction per cycle.
+    fp32 = None
+    if fp32_inst:
+        fp32_peak = 148 * 128 * mhz * 1e6
+        fp32_achieved = fp32_inst / (kern[dom] / 1e3)
+        fp32 = {"kernel": dom, "fp32_thread_instructions_per_launch": fp32_inst,
+                "achieved": fp32_achieved, "peak": fp32_peak, "unit": "thread-inst/s",
+                "frac": fp32_achieved / fp32_peak,
+                "source": "instruction count from profiles/traffic.json (ncu)"}
 
     if rank == 0:
         cpu = None
@@ -801,6 +814,7 @@ def run_gpu(args) -> None:
                          "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,
                          "launch_ms": kern[dom]},
             "issue_roofline": issue,
+            "fp32_roofline": fp32,
             "kernel_ms": kern,
             "step_roofline": {"algorithmic_bytes_per_step": step_bytes(it_total, head["passes"]) * n,
                               "frac": step_bytes(it_total, head["passes"]) * n
