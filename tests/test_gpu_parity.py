@@ -329,6 +329,25 @@ def test_frames_bit_exact_1m_tolerance(oracle_mod):
     assert st.density_iterations >= 1 and st.divergence_iterations >= 1
 
 
+def test_frames_bit_exact_4m_tolerance(oracle_mod):
+    """The benchmarked 4M dam break (256x64x256 lattice, FIXED mode, the
+    tolerance solver): the 2^22-slot hash table, a 22-bit radix key and the
+    FP64 residual sums over 16384 chunks; 2 frames from rest, every field and
+    every stats word.  The first frames from rest need 19 + 14 iterations,
+    which would take the oracle minutes at this size, so the iteration cap is
+    4: both solves stop at the cap above the 0.1 % tolerance."""
+    w = scene.workload("dam_break_4m")
+    p = _abi.copy_params(w.params)
+    p.max_iterations = 4
+    pos = w.positions()
+    sim, orc, st = _run_frames(oracle_mod, p, pos, frames=2)
+    assert pos.shape[0] == 1 << 22
+    assert sim.data.table_size == 1 << 22
+    assert st.density_iterations == 4 and st.divergence_iterations == 4
+    assert st.density_residual > p.density_tolerance
+    sim.close()
+
+
 def test_frames_bit_exact_262k_adaptive_cfl(oracle_mod):
     """The 262k dam break with adaptive CFL and the tolerance solver: 3
     frames (dt changes every frame on the device)."""
